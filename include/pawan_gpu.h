@@ -1,0 +1,152 @@
+/*
+ * pawan_gpu.h - C ABI of the B200 vortex-particle backend.
+ *
+ * This is the boundary a PAWAN build binds to replace the CPU solve of its
+ * __interaction / __parallel backend and the stage loop of its __rk3 / __rk4
+ * integrators.  Plain C types only (no CUDA or torch types); every entry point
+ * returns PGPU_OK (0) or a negative PGPU_E* code, and pgpu_last_error() gives
+ * the message of the last failure on a context.
+ *
+ * Units and layouts follow PAWAN's __wake (src/wake/wake.h:49-54): positions
+ * and strengths are row-major (n, 3) FP64 host arrays, radii and volumes (n).
+ *
+ * A context owns all device memory and one CUDA stream; it is used from one
+ * host thread at a time (PAWAN calls its solver from one thread).  Wakes are
+ * grouped into systems: the wakes of one system all interact with one another,
+ * exactly as the wakes held by one PAWAN __interaction do
+ * (src/interaction/interaction.cpp:196-210); different systems are independent
+ * and are advanced together in one persistent launch per stage.
+ */
+#ifndef PAWAN_GPU_H_
+#define PAWAN_GPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGPU_OK 0
+#define PGPU_EINVAL (-1)   /* bad argument or call order */
+#define PGPU_ENOMEM (-2)   /* device or host allocation failed */
+#define PGPU_ECUDA (-3)    /* a CUDA call failed */
+#define PGPU_ETIMEOUT (-4) /* a bounded device wait expired */
+#define PGPU_ENUMERIC (-5) /* a non-finite value was produced */
+
+#define PGPU_FP32C 0 /* FP32 pair terms, compensated per-target sums, FP64 state */
+#define PGPU_FP64 1  /* FP64 throughout */
+
+#define PGPU_EULER 0
+#define PGPU_RK3 1
+#define PGPU_RK4 2
+
+typedef struct pgpu_ctx pgpu_ctx;
+
+typedef struct pgpu_config {
+  int precision;   /* PGPU_FP32C or PGPU_FP64 */
+  int device;      /* CUDA device ordinal */
+  double nu;       /* kinematic viscosity (PAWAN's protected __interaction::_nu, interaction.h:25) */
+  double vinf[3];  /* uniform inflow added after each step, x += vinf dt
+                      (__wake::updateVinfEffect, wake.cpp:564-577, called from integration.cpp:172) */
+  int block;       /* pair-kernel threads per CTA; 0 = autotuned default */
+  int tpt;         /* pair-kernel targets per thread; 0 = autotuned default */
+  int chunks;      /* source chunks per system (1..16); 0 = automatic */
+  int use_graphs;  /* capture each time step in a CUDA graph (default 1) */
+} pgpu_config;
+
+/* Fills cfg with defaults (FP32C, device 0, nu = 1.56e-5 as __interaction(),
+ * interaction.cpp:15, no inflow, tuned tiles, graphs on). */
+void pgpu_config_default(pgpu_config *cfg);
+
+/* Replaces: constructing a backend, `new pawan::__parallel(W)` (src/pawan.cpp:48,
+ * src/interaction/parallel.cpp:11-12). */
+int pgpu_create(pgpu_ctx **ctx, const pgpu_config *cfg);
+/* Replaces: the backend destructor (interaction.cpp:37-42). */
+int pgpu_destroy(pgpu_ctx *ctx);
+
+/* Replaces: __interaction::addWake (interaction.h:198, interaction.cpp:44-52).
+ * Reserves `capacity` particle slots for a wake of system `system`.  Wakes must
+ * be added before the first particle upload.  Within a system every wake but
+ * the last must be full (n == capacity) when the system is solved; the last
+ * wake may grow up to its capacity (pgpu_append_particles). */
+int pgpu_add_wake(pgpu_ctx *ctx, int32_t system, int64_t capacity, int32_t *wake_id);
+
+/* Replaces: filling __wake::_position/_vorticity/_radius/_volume
+ * (wake.h:49-54) - uploads n particles (host buffers) into a wake. */
+int pgpu_set_particles(pgpu_ctx *ctx, int32_t wake, int64_t n, const double *pos, const double *alpha,
+                       const double *sigma, const double *vol);
+/* Replaces: __wake::addParticles (wake.cpp:179-531 in the coupled run) for a
+ * synthetic shedder - appends m particles to the last wake of a system. */
+int pgpu_append_particles(pgpu_ctx *ctx, int32_t wake, int64_t m, const double *pos, const double *alpha,
+                          const double *sigma, const double *vol);
+int pgpu_get_num_particles(pgpu_ctx *ctx, int32_t wake, int64_t *n);
+
+/* Replaces: __interaction::getStates (interaction.cpp:357-365) restricted to
+ * one wake: downloads positions and strengths (n, 3) each. */
+int pgpu_get_state(pgpu_ctx *ctx, int32_t wake, double *pos, double *alpha);
+
+/* Replaces: __interaction::setStates / getStates on PAWAN's flat state vector
+ * (interaction.cpp:337-365; per wake [x (maxN x 3) ; alpha (maxN x 3)] at an
+ * offset of sum 6 maxN, wake.cpp:856-893).  `maxn` lists each wake's PAWAN
+ * capacity (__wake::_maxnumParticles), in wake-id order. */
+int pgpu_set_states_flat(pgpu_ctx *ctx, const double *state, const int64_t *maxn, int32_t nwakes);
+int pgpu_get_states_flat(pgpu_ctx *ctx, double *state, const int64_t *maxn, int32_t nwakes);
+/* Replaces: __interaction::getRates (interaction.cpp:347-355): the flat rate
+ * vector [velocity ; dalpha/dt] of the last evaluation. */
+int pgpu_get_rates_flat(pgpu_ctx *ctx, double *rate, const int64_t *maxn, int32_t nwakes);
+
+/* Replaces: __interaction::solve (interaction.cpp:54-57) with the OpenMP pair
+ * loops of __parallel::interact (parallel.cpp:14-86): one rate evaluation of
+ * every system at its current state. */
+int pgpu_solve(pgpu_ctx *ctx);
+/* Replaces: __interaction::getRates restricted to one wake: velocity and
+ * dalpha/dt of the last evaluation, (n, 3) each. */
+int pgpu_get_rates(pgpu_ctx *ctx, int32_t wake, double *vel, double *dalpha);
+
+/* Replaces: the time loop body of __integration::integrate
+ * (integration.cpp:112-116) with __rk4::step (rk4.cpp:12-77), __rk3::step
+ * (rk3.cpp:12-65) or the Euler step (integration.cpp:198-208): advances every
+ * system nsteps steps on the device; the config's vinf is applied after each
+ * step.  The state stays on the device. */
+int pgpu_step(pgpu_ctx *ctx, int scheme, double dt, int32_t nsteps);
+
+/* Replaces: __interaction::diagnose (interaction.cpp:64-194) for one system.
+ * out[15] = total vorticity(3), linear impulse(3), angular impulse(3),
+ * helicity, enstrophy, enstrophyF, kinetic energy, kinetic energyF, Zc - the
+ * record of writediagnosis (interaction.cpp:325-335); vbi[3] = velocity
+ * induced at the origin (may be NULL).  Enstrophy terms are identically zero
+ * for the Gaussian kernel (gaussian.h:69-92).  Zc follows PAWAN: the last wake
+ * with non-zero weight wins, else the previous value is kept. */
+int pgpu_diagnose(pgpu_ctx *ctx, int32_t system, double *out, double *vbi);
+
+/* Replaces: __interaction::getVi (interaction.cpp:453-477) and the airstation
+ * loop of getInflow (:399-451): velocity induced at npts points (row-major
+ * (npts, 3)) by every particle of a system, using each particle's own radius. */
+int pgpu_probe(pgpu_ctx *ctx, int32_t system, int64_t npts, const double *pts, double *vel);
+
+/* Waits for all queued work; reports PGPU_ENUMERIC if a step produced a
+ * non-finite state. */
+int pgpu_sync(pgpu_ctx *ctx);
+
+/* Device time in milliseconds of the pair kernel launches since the last call
+ * (CUDA events on the context stream), and the number of them. */
+int pgpu_pair_kernel_time(pgpu_ctx *ctx, double *ms, int64_t *launches);
+
+/* Kernel launches issued since context creation (all kernels of this library). */
+int64_t pgpu_launch_count(pgpu_ctx *ctx);
+
+/* Times every compiled pair-kernel shape on the current particles (`reps`
+ * launches each) and selects the fastest for subsequent solves and steps.
+ * block/tpt receive the choice; ms_per_launch (may be NULL) receives the
+ * time of each candidate in the order of pgpu_kernel_shapes. */
+int pgpu_autotune(pgpu_ctx *ctx, int reps, int *block, int *tpt, double *ms_per_launch);
+/* Number of compiled pair-kernel shapes and their (block, tpt). */
+int pgpu_kernel_shapes(int *block, int *tpt, int max);
+
+const char *pgpu_last_error(pgpu_ctx *ctx);
+const char *pgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,230 @@
+/*
+ * FP64 CPU restatement of PAWAN's vortex-particle hot path (see restate.h).
+ * TEST INFRASTRUCTURE ONLY.
+ *
+ * Each function cites the PAWAN code it restates.  Differences in structure:
+ * PAWAN visits every unordered pair once and applies it to both ends
+ * (src/interaction/parallel.cpp:14-49); here every target sums over all
+ * sources (ordered pairs), which is the same sum in a different order, with no
+ * per-pair heap allocation, parallel over targets with OpenMP.
+ */
+#include "restate.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* Gaussian regularisation, src/interaction/gaussian.h:20-60 (ZETASIG, QSIG,
+ * KERNEL): rb = rho/sigma,
+ *   zeta = exp(-rb^2/2) / (sigma^3 (2 pi)^(3/2))
+ *   phi  = erf(rb / sqrt 2) / (4 pi sigma^3)
+ *   q    = (phi/rb - zeta) / rb^2
+ *   F    = (zeta - 3 q) / rho^2
+ * The diffusion kernel eta is zeta itself (gaussian.h:58). */
+static inline void kernel_terms(double rho, double sigma, double *q, double *F, double *Z) {
+  const double rb = rho / sigma;
+  const double s3 = sigma * sigma * sigma;
+  const double z = exp(-0.5 * rb * rb) / s3 / pow(2.0 * M_PI, 1.5);
+  const double phi = 0.25 / M_PI * erf(rb / sqrt(2.0)) / s3;
+  const double qq = (phi / rb - z) / (rb * rb);
+  *q = qq;
+  *Z = z;
+  *F = (z - 3.0 * qq) / (rho * rho);
+}
+
+static inline void cross3(const double *a, const double *b, double *c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* One target t summed over all sources s != t.  Per ordered pair (target t,
+ * source s), with d = x_t - x_s and sigma_ts = sqrt((s_s^2 + s_t^2)/2)
+ * (interaction_utils.h:547):
+ *   velocity   u_t  += q (alpha_s x d)                 (VELOCITY :55-62)
+ *   stretching da_t += q (a_t x a_s) + F [d.(a_t x a_s)] d   (VORSTRETCH :73-105)
+ *   diffusion  da_t += nu zeta / (sigma^2/2) (vol_t a_s - vol_s a_t)  (DIFFUSION :344-378)
+ * The source side of PAWAN's symmetric update (-q(a_t x d), -da) is the same
+ * expression with the roles swapped (INTERACT :523-576). */
+static void rates_one(int64_t t, int64_t n, const double *pos, const double *alpha,
+                      const double *sigma, const double *vol, double nu, double *v, double *da) {
+  const double *xt = pos + 3 * t, *at = alpha + 3 * t;
+  const double st = sigma[t], vt = vol[t];
+  double u0 = 0, u1 = 0, u2 = 0, d0 = 0, d1 = 0, d2 = 0;
+  for (int64_t s = 0; s < n; ++s) {
+    if (s == t) continue;
+    const double *xs = pos + 3 * s, *as = alpha + 3 * s;
+    const double d[3] = {xt[0] - xs[0], xt[1] - xs[1], xt[2] - xs[2]};
+    const double rho = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const double sg = sqrt(0.5 * (sigma[s] * sigma[s] + st * st));
+    double q, F, Z;
+    kernel_terms(rho, sg, &q, &F, &Z);
+    double w[3];
+    cross3(as, d, w);
+    u0 += q * w[0]; u1 += q * w[1]; u2 += q * w[2];
+    double c[3];
+    cross3(at, as, c);
+    const double dc = d[0] * c[0] + d[1] * c[1] + d[2] * c[2];
+    const double k = nu * Z / (0.5 * sg * sg);
+    const double vs = vol[s];
+    d0 += q * c[0] + F * dc * d[0] + k * (vt * as[0] - vs * at[0]);
+    d1 += q * c[1] + F * dc * d[1] + k * (vt * as[1] - vs * at[1]);
+    d2 += q * c[2] + F * dc * d[2] + k * (vt * as[2] - vs * at[2]);
+  }
+  v[0] = u0; v[1] = u1; v[2] = u2;
+  da[0] = d0; da[1] = d1; da[2] = d2;
+}
+
+void rs_rates(int64_t n, const double *pos, const double *alpha, const double *sigma,
+              const double *vol, double nu, const int64_t *targets, int64_t nt,
+              double *vel, double *dalpha) {
+  if (!targets) nt = n;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < nt; ++i) {
+    const int64_t t = targets ? targets[i] : i;
+    rates_one(t, n, pos, alpha, sigma, vol, nu, vel + 3 * i, dalpha + 3 * i);
+  }
+}
+
+/* Time stepping on the packed state [x ; alpha] (the flat FP64 vector of
+ * __wake::getStates, wake.cpp:882-893).
+ *   Euler (integration.cpp:198-208): x += dt k1
+ *   RK3   (rk3.cpp:12-65, Kutta):  x1 = x + dt/2 k1, x2 = x - dt k1 + 2 dt k2,
+ *                                  x += dt/6 k1 + 2dt/3 k2 + dt/6 k3
+ *   RK4   (rk4.cpp:12-77):         x1 = x + dt/2 k1, x2 = x + dt/2 k2,
+ *                                  x3 = x + dt k3,
+ *                                  x += dt/6 (k1 + k4) + dt/3 (k2 + k3) */
+static void eval(int64_t n, const double *st, const double *sigma, const double *vol, double nu,
+                 double *k) {
+  rs_rates(n, st, st + 3 * n, sigma, vol, nu, NULL, n, k, k + 3 * n);
+}
+
+void rs_step(int scheme, double dt, int nsteps, int64_t n, double *pos, double *alpha,
+             const double *sigma, const double *vol, double nu) {
+  const int64_t m = 6 * n;
+  double *x = (double *)malloc(sizeof(double) * m);
+  double *y = (double *)malloc(sizeof(double) * m);
+  double *k1 = (double *)malloc(sizeof(double) * m);
+  double *k2 = (double *)malloc(sizeof(double) * m);
+  double *k3 = (double *)malloc(sizeof(double) * m);
+  double *k4 = (double *)malloc(sizeof(double) * m);
+  memcpy(x, pos, sizeof(double) * 3 * n);
+  memcpy(x + 3 * n, alpha, sizeof(double) * 3 * n);
+  for (int it = 0; it < nsteps; ++it) {
+    eval(n, x, sigma, vol, nu, k1);
+    if (scheme == 0) {
+      for (int64_t i = 0; i < m; ++i) x[i] += dt * k1[i];
+    } else if (scheme == 1) {
+      for (int64_t i = 0; i < m; ++i) y[i] = x[i] + 0.5 * dt * k1[i];
+      eval(n, y, sigma, vol, nu, k2);
+      for (int64_t i = 0; i < m; ++i) y[i] = (x[i] + 2.0 * dt * k2[i]) - dt * k1[i];
+      eval(n, y, sigma, vol, nu, k3);
+      for (int64_t i = 0; i < m; ++i)
+        x[i] += (dt * k1[i] / 6.0 + dt / 6.0 * k3[i]) + dt * 2.0 / 3.0 * k2[i];
+    } else {
+      for (int64_t i = 0; i < m; ++i) y[i] = x[i] + 0.5 * dt * k1[i];
+      eval(n, y, sigma, vol, nu, k2);
+      for (int64_t i = 0; i < m; ++i) y[i] = x[i] + 0.5 * dt * k2[i];
+      eval(n, y, sigma, vol, nu, k3);
+      for (int64_t i = 0; i < m; ++i) y[i] = x[i] + dt * k3[i];
+      eval(n, y, sigma, vol, nu, k4);
+      for (int64_t i = 0; i < m; ++i)
+        x[i] += (k1[i] + k4[i]) * (dt / 6.0) + (k2[i] + k3[i]) * (dt / 3.0);
+    }
+  }
+  memcpy(pos, x, sizeof(double) * 3 * n);
+  memcpy(alpha, x + 3 * n, sizeof(double) * 3 * n);
+  free(x); free(y); free(k1); free(k2); free(k3); free(k4);
+}
+
+/* Diagnostics, src/interaction/interaction.cpp:64-194 with the OpenMP bodies
+ * of parallel.cpp:140-401 and the pair terms of interaction_utils.h:214-331:
+ *   total vorticity  sum alpha
+ *   linear impulse   1/2 sum x x alpha
+ *   angular impulse  1/3 sum x x (x x alpha)
+ *   helicity         sum_{i != j} q(rho, s_ij) (x_j - x_i).(a_i x a_j)
+ *   enstrophy[F]     0 for the Gaussian kernel (gaussian.h:69-92)
+ *   KE   = sum_i |a_i|^2/(8 pi s_i)
+ *        + sum_{i != j} [(rho^2 + 2 s^2)(a_i.a_j) + (d.a_i)(d.a_j)] / (16 pi (rho^2 + s^2)^(3/2))
+ *   KEF  = sum_i 3|a_i|^2/(16 pi s_i)
+ *        + sum_{i != j} (rho^2 + 1.5 s^2)(a_i.a_j) / (8 pi (rho^2 + s^2)^(3/2))
+ * with s^2 = (s_i^2 + s_j^2)/2.  Zc (interaction.cpp:135-157) takes the last
+ * wake with a non-zero weight; vbi is getVi at the origin (:184-193). */
+void rs_diagnose(int nw, const int64_t *offsets, const double *pos, const double *alpha,
+                 const double *sigma, double zc_prev, double *out, double *vbi) {
+  const int64_t n = offsets[nw];
+  double O[3] = {0, 0, 0}, I[3] = {0, 0, 0}, A[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i) {
+    const double *x = pos + 3 * i, *a = alpha + 3 * i;
+    double xa[3], xxa[3];
+    cross3(x, a, xa);
+    cross3(x, xa, xxa);
+    for (int k = 0; k < 3; ++k) { O[k] += a[k]; I[k] += xa[k]; A[k] += xxa[k]; }
+  }
+  double H = 0, KE = 0, KEF = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : H, KE, KEF)
+  for (int64_t i = 0; i < n; ++i) {
+    const double *xi = pos + 3 * i, *ai = alpha + 3 * i;
+    const double si = sigma[i];
+    const double a2 = ai[0] * ai[0] + ai[1] * ai[1] + ai[2] * ai[2];
+    double h = 0, ke = a2 / si / 8.0 / M_PI, kef = 3.0 * a2 / (si * 16.0) / M_PI;
+    for (int64_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const double *xj = pos + 3 * j, *aj = alpha + 3 * j;
+      const double d[3] = {xj[0] - xi[0], xj[1] - xi[1], xj[2] - xi[2]};
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      const double s2 = 0.5 * (si * si + sigma[j] * sigma[j]);
+      double q, F, Z;
+      kernel_terms(sqrt(r2), sqrt(s2), &q, &F, &Z);
+      double c[3];
+      cross3(ai, aj, c);
+      h += q * (d[0] * c[0] + d[1] * c[1] + d[2] * c[2]);
+      const double aa = ai[0] * aj[0] + ai[1] * aj[1] + ai[2] * aj[2];
+      const double dai = d[0] * ai[0] + d[1] * ai[1] + d[2] * ai[2];
+      const double daj = d[0] * aj[0] + d[1] * aj[1] + d[2] * aj[2];
+      const double den = pow(r2 + s2, 1.5);
+      ke += ((r2 + 2.0 * s2) * aa + dai * daj) / den / 16.0 / M_PI;
+      kef += (r2 + 1.5 * s2) * aa / den / 8.0 / M_PI;
+    }
+    H += h; KE += ke; KEF += kef;
+  }
+  double zc = zc_prev;
+  for (int w = 0; w < nw; ++w) {
+    double num = 0, den = 0;
+    for (int64_t i = offsets[w]; i < offsets[w + 1]; ++i) {
+      const double *x = pos + 3 * i, *a = alpha + 3 * i;
+      const double om = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+      const double rr = x[0] * x[0] + x[1] * x[1];
+      num += om * x[2] * rr;
+      den += om * rr;
+    }
+    if (den != 0.0) zc = num / den;
+  }
+  for (int k = 0; k < 3; ++k) { out[k] = O[k]; out[3 + k] = 0.5 * I[k]; out[6 + k] = A[k] / 3.0; }
+  out[9] = H; out[10] = 0.0; out[11] = 0.0; out[12] = KE; out[13] = KEF; out[14] = zc;
+  const double origin[3] = {0, 0, 0};
+  rs_getvi(n, pos, alpha, sigma, origin, vbi);
+}
+
+/* __interaction::getVi (interaction.cpp:453-477): d = r - x_i, the particle's
+ * own radius, u += q (alpha_i x d). */
+void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *sigma,
+              const double *r, double *out) {
+  double u[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i) {
+    const double d[3] = {r[0] - pos[3 * i], r[1] - pos[3 * i + 1], r[2] - pos[3 * i + 2]};
+    const double rho = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    double q, F, Z, w[3];
+    kernel_terms(rho, sigma[i], &q, &F, &Z);
+    cross3(alpha + 3 * i, d, w);
+    for (int k = 0; k < 3; ++k) u[k] += q * w[k];
+  }
+  for (int k = 0; k < 3; ++k) out[k] = u[k];
+}
+
+int rs_threads(void) { return omp_get_max_threads(); }

@@ -1,0 +1,255 @@
+"""ctypes binding of the C ABI in ``include/pawan_gpu.h``.
+
+The product path is ``lib/libpawan_gpu.so`` (built by ``pawan_b200.build``).
+There is no CPU fallback: if the library or a GPU is missing, loading fails
+with an exception.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+PGPU_OK = 0
+PGPU_EINVAL = -1
+PGPU_ENOMEM = -2
+PGPU_ECUDA = -3
+PGPU_ETIMEOUT = -4
+PGPU_ENUMERIC = -5
+
+FP32C = 0
+FP64 = 1
+EULER, RK3, RK4 = 0, 1, 2
+SCHEMES = {"euler": EULER, "rk3": RK3, "rk4": RK4}
+
+# Entry points declared in include/pawan_gpu.h (checked by the CPU tests).
+EXPORTS = [
+    "pgpu_config_default", "pgpu_create", "pgpu_destroy", "pgpu_add_wake", "pgpu_set_particles",
+    "pgpu_append_particles", "pgpu_get_num_particles", "pgpu_get_state", "pgpu_set_states_flat",
+    "pgpu_get_states_flat", "pgpu_get_rates_flat", "pgpu_solve", "pgpu_get_rates", "pgpu_step",
+    "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
+    "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version",
+]
+
+
+class PgpuConfig(C.Structure):
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("nu", C.c_double), ("vinf", C.c_double * 3),
+                ("block", C.c_int), ("tpt", C.c_int), ("chunks", C.c_int), ("use_graphs", C.c_int)]
+
+
+class PgpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pawan_gpu error {code}: {msg}")
+        self.code = code
+
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_lib = None
+
+
+def lib_path() -> Path:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = False):
+    """Loads libpawan_gpu.so (raises if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = lib_path()
+    if not p.exists():
+        if build_if_missing:
+            _build.build()
+        else:
+            raise RuntimeError(f"{p} is missing: run `python -m pawan_b200.build`")
+    lib = C.CDLL(str(p))
+    vp = C.c_void_p
+    sig = {
+        "pgpu_config_default": (None, [C.POINTER(PgpuConfig)]),
+        "pgpu_create": (C.c_int, [C.POINTER(vp), C.POINTER(PgpuConfig)]),
+        "pgpu_destroy": (C.c_int, [vp]),
+        "pgpu_add_wake": (C.c_int, [vp, C.c_int32, C.c_int64, C.POINTER(C.c_int32)]),
+        "pgpu_set_particles": (C.c_int, [vp, C.c_int32, C.c_int64, _dp, _dp, _dp, _dp]),
+        "pgpu_append_particles": (C.c_int, [vp, C.c_int32, C.c_int64, _dp, _dp, _dp, _dp]),
+        "pgpu_get_num_particles": (C.c_int, [vp, C.c_int32, _i64p]),
+        "pgpu_get_state": (C.c_int, [vp, C.c_int32, _dp, _dp]),
+        "pgpu_set_states_flat": (C.c_int, [vp, _dp, _i64p, C.c_int32]),
+        "pgpu_get_states_flat": (C.c_int, [vp, _dp, _i64p, C.c_int32]),
+        "pgpu_get_rates_flat": (C.c_int, [vp, _dp, _i64p, C.c_int32]),
+        "pgpu_solve": (C.c_int, [vp]),
+        "pgpu_get_rates": (C.c_int, [vp, C.c_int32, _dp, _dp]),
+        "pgpu_step": (C.c_int, [vp, C.c_int, C.c_double, C.c_int32]),
+        "pgpu_diagnose": (C.c_int, [vp, C.c_int32, _dp, _dp]),
+        "pgpu_probe": (C.c_int, [vp, C.c_int32, C.c_int64, _dp, _dp]),
+        "pgpu_sync": (C.c_int, [vp]),
+        "pgpu_pair_kernel_time": (C.c_int, [vp, _dp, _i64p]),
+        "pgpu_launch_count": (C.c_int64, [vp]),
+        "pgpu_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+        "pgpu_kernel_shapes": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
+        "pgpu_last_error": (C.c_char_p, [vp]),
+        "pgpu_version": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def kernel_shapes() -> list[tuple[int, int]]:
+    lib = load()
+    b = (C.c_int * 32)()
+    t = (C.c_int * 32)()
+    n = lib.pgpu_kernel_shapes(b, t, 32)
+    return [(b[i], t[i]) for i in range(n)]
+
+
+class Context:
+    """One backend context: wakes grouped into systems, all device-resident."""
+
+    def __init__(self, precision: int = FP32C, nu: float = 1.56e-5, device: int = 0, vinf=(0.0, 0.0, 0.0),
+                 block: int = 0, tpt: int = 0, chunks: int = 0, use_graphs: bool = True):
+        self.lib = load()
+        cfg = PgpuConfig()
+        self.lib.pgpu_config_default(C.byref(cfg))
+        cfg.precision = precision
+        cfg.device = device
+        cfg.nu = nu
+        for k in range(3):
+            cfg.vinf[k] = float(vinf[k])
+        cfg.block, cfg.tpt, cfg.chunks = block, tpt, chunks
+        cfg.use_graphs = 1 if use_graphs else 0
+        h = C.c_void_p()
+        rc = self.lib.pgpu_create(C.byref(h), C.byref(cfg))
+        if rc != PGPU_OK:
+            raise PgpuError(rc, "pgpu_create failed")
+        self.h = h
+        self.wake_sizes: list[int] = []
+        self.wake_system: list[int] = []
+
+    def _ck(self, rc: int):
+        if rc != PGPU_OK:
+            raise PgpuError(rc, self.lib.pgpu_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------ wakes
+    def add_wake(self, capacity: int, system: int = 0) -> int:
+        wid = C.c_int32()
+        self._ck(self.lib.pgpu_add_wake(self.h, system, int(capacity), C.byref(wid)))
+        self.wake_sizes.append(0)
+        self.wake_system.append(system)
+        return wid.value
+
+    def set_particles(self, wake: int, w):
+        arr = [_c(w.pos), _c(w.alpha), _c(w.sigma), _c(w.vol)]
+        self._ck(self.lib.pgpu_set_particles(self.h, wake, w.n, *[_p(a) for a in arr]))
+        self.wake_sizes[wake] = w.n
+
+    def append_particles(self, wake: int, w):
+        arr = [_c(w.pos), _c(w.alpha), _c(w.sigma), _c(w.vol)]
+        self._ck(self.lib.pgpu_append_particles(self.h, wake, w.n, *[_p(a) for a in arr]))
+        self.wake_sizes[wake] += w.n
+
+    def num_particles(self, wake: int) -> int:
+        n = C.c_int64()
+        self._ck(self.lib.pgpu_get_num_particles(self.h, wake, C.byref(n)))
+        return n.value
+
+    def state(self, wake: int = 0, out=None):
+        n = self.num_particles(wake)
+        if out is None:
+            out = (np.zeros((n, 3)), np.zeros((n, 3)))
+        self._ck(self.lib.pgpu_get_state(self.h, wake, _p(out[0]), _p(out[1])))
+        return out
+
+    def rates(self, wake: int = 0):
+        n = self.num_particles(wake)
+        v, a = np.zeros((n, 3)), np.zeros((n, 3))
+        self._ck(self.lib.pgpu_get_rates(self.h, wake, _p(v), _p(a)))
+        return v, a
+
+    # ------------------------------------------------------------ solve / step
+    def solve(self):
+        self._ck(self.lib.pgpu_solve(self.h))
+
+    def step(self, scheme: str | int, dt: float, nsteps: int = 1):
+        s = SCHEMES[scheme] if isinstance(scheme, str) else scheme
+        self._ck(self.lib.pgpu_step(self.h, s, float(dt), int(nsteps)))
+
+    def sync(self):
+        self._ck(self.lib.pgpu_sync(self.h))
+
+    def diagnose(self, system: int = 0):
+        out = np.zeros(15)
+        vbi = np.zeros(3)
+        self._ck(self.lib.pgpu_diagnose(self.h, system, _p(out), _p(vbi)))
+        return out, vbi
+
+    def probe(self, pts, system: int = 0) -> np.ndarray:
+        pts = _c(pts).reshape(-1, 3)
+        vel = np.zeros_like(pts)
+        self._ck(self.lib.pgpu_probe(self.h, system, pts.shape[0], _p(pts), _p(vel)))
+        return vel
+
+    def pair_kernel_time(self) -> tuple[float, int]:
+        ms = C.c_double()
+        n = C.c_int64()
+        self._ck(self.lib.pgpu_pair_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def launch_count(self) -> int:
+        return int(self.lib.pgpu_launch_count(self.h))
+
+    def autotune(self, reps: int = 2):
+        b, t = C.c_int(), C.c_int()
+        ms = np.zeros(32)
+        self._ck(self.lib.pgpu_autotune(self.h, reps, C.byref(b), C.byref(t), _p(ms)))
+        shapes = kernel_shapes()
+        return (b.value, t.value), {shapes[i]: float(ms[i]) for i in range(len(shapes))}
+
+    # ------------------------------------------------------------ PAWAN flat state vector
+    def set_states_flat(self, state, maxn):
+        m = np.ascontiguousarray(maxn, dtype=np.int64)
+        st = _c(state)
+        self._ck(self.lib.pgpu_set_states_flat(self.h, _p(st), m.ctypes.data_as(_i64p), len(m)))
+
+    def get_states_flat(self, maxn):
+        m = np.ascontiguousarray(maxn, dtype=np.int64)
+        st = np.zeros(int(6 * m.sum()))
+        self._ck(self.lib.pgpu_get_states_flat(self.h, _p(st), m.ctypes.data_as(_i64p), len(m)))
+        return st
+
+    def get_rates_flat(self, maxn):
+        m = np.ascontiguousarray(maxn, dtype=np.int64)
+        st = np.zeros(int(6 * m.sum()))
+        self._ck(self.lib.pgpu_get_rates_flat(self.h, _p(st), m.ctypes.data_as(_i64p), len(m)))
+        return st

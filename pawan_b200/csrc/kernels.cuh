@@ -1,0 +1,561 @@
+// Device kernels of the B200 vortex-particle path.
+//
+//   pair_kernel     all-pairs velocity / stretching / diffusion rates
+//                   (PAWAN __parallel::interact, src/interaction/parallel.cpp:14-86,
+//                   per-pair INTERACT, interaction_utils.h:523-576)
+//   stage_kernel    RK3 / RK4 / Euler stage updates on the FP64 state, fused with
+//                   the reduction of the per-chunk partial rates and the repack of
+//                   the next stage's source records (src/integration/rk4.cpp:12-77,
+//                   rk3.cpp:12-65, integration.cpp:198-208)
+//   diag_pair_kernel / diag_wake_kernel
+//                   conserved-quantity diagnostics (interaction.cpp:64-194,
+//                   parallel.cpp:140-401)
+//   scatter / gather / pack kernels for the host row-major <-> device SoA layout.
+//
+// Work decomposition of the O(N^2) kernels.  Each system (one PAWAN
+// __interaction: all of its particles interact) is cut into target tiles of
+// TT = BLOCK * TPT particles and NCH source chunks.  A work item is one
+// (system, tile, chunk); items of all systems form one list ordered by
+// decreasing system size, and a persistent grid (a few CTAs per SM) takes items
+// from an atomic counter.  Every item writes compensated per-target partial
+// sums for its chunk to partial[chunk][component][particle] (FP64); the next
+// stage kernel adds the NCH partials in a fixed order, so results are
+// bit-reproducible run to run.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pair_math.cuh"
+
+namespace pgpu {
+
+constexpr int kMaxChunks = 16;
+constexpr int kDiagFields = 19;
+
+// One system in the work list (sorted by decreasing work).
+struct PlanEntry {
+  int64_t off;         // first particle slot of the system
+  int64_t n;           // particles in the system
+  int64_t item_start;  // first work item of the system
+  int64_t tiles;       // target tiles
+  int64_t chunk;       // sources per chunk (multiple of the source tile)
+};
+
+template <typename T> struct PairArgs {
+  const v4_t<T> *P;  // (x, y, z, sigma^2/2)
+  const v4_t<T> *Q;  // (alpha, volume)
+  double *partial;   // [nch][6][cap]
+  const PlanEntry *plan;
+  int nsys;
+  int nch;
+  int64_t cap;
+  T nu2;  // 2 nu
+  unsigned int *counters;  // [0] next item, [1] finished CTAs
+};
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <typename T> __device__ __forceinline__ v4_t<T> make_v4(T a, T b, T c, T d);
+template <> __device__ __forceinline__ float4 make_v4<float>(float a, float b, float c, float d) {
+  return make_float4(a, b, c, d);
+}
+template <> __device__ __forceinline__ double4 make_v4<double>(double a, double b, double c, double d) {
+  return make_double4(a, b, c, d);
+}
+
+// Copy one packed record (16 B for FP32, 32 B for FP64) with cp.async.
+template <typename T> __device__ __forceinline__ void cp_record(v4_t<T> *dst, const v4_t<T> *src) {
+  if constexpr (sizeof(v4_t<T>) == 16) {
+    cp_async16(dst, src);
+  } else {
+    cp_async16(dst, src);
+    cp_async16(reinterpret_cast<char *>(dst) + 16, reinterpret_cast<const char *>(src) + 16);
+  }
+}
+
+// A padding source: far away, zero strength, zero volume.  Every term it adds
+// is an exact zero and no term overflows (rho^2 ~ 3e36 < FLT_MAX).
+template <typename T> __device__ __forceinline__ v4_t<T> pad_P() { return make_v4<T>(T(1e18), T(1e18), T(1e18), T(1)); }
+template <typename T> __device__ __forceinline__ v4_t<T> pad_Q() { return make_v4<T>(T(0), T(0), T(0), T(0)); }
+
+__device__ __forceinline__ int find_plan(const PlanEntry *plan, int nsys, int64_t item) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (plan[mid].item_start <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Persistent CTA item loop shared by the O(N^2) kernels.  Returns false when
+// the list is exhausted; the last CTA to leave resets the counters so the
+// kernel can be relaunched (or replayed from a CUDA graph) with no memset.
+__device__ __forceinline__ bool next_item(unsigned int *counters, int64_t total, int64_t &item, int *s_item) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_item = (int)atomicAdd(&counters[0], 1u);
+  __syncthreads();
+  item = *s_item;
+  if (item < total) return true;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned done = atomicAdd(&counters[1], 1u);
+    if (done == gridDim.x - 1) {
+      counters[0] = 0u;
+      counters[1] = 0u;
+      __threadfence();
+    }
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------- pair kernel
+// BLOCK threads, TPT targets per thread, TILE sources per shared-memory tile
+// (TILE == BLOCK: each thread stages one record), CG sources per compensation
+// group (plain FP32 partial sums over CG sources, then an error-free two-sum
+// into the per-target (hi, lo) accumulators).
+template <typename T, int BLOCK, int TPT, int CG>
+__global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
+  constexpr int TILE = BLOCK;
+  constexpr int TT = BLOCK * TPT;
+  static_assert(TILE % CG == 0, "compensation group must divide the tile");
+  __shared__ __align__(16) v4_t<T> sP[2][TILE];
+  __shared__ __align__(16) v4_t<T> sQ[2][TILE];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const int64_t total = a.plan[a.nsys].item_start;
+  int64_t item;
+  while (next_item(a.counters, total, item, &s_item)) {
+    const int si = find_plan(a.plan, a.nsys, item);
+    const PlanEntry pe = a.plan[si];
+    const int64_t local = item - pe.item_start;
+    const int64_t tile = local / a.nch;
+    const int c = (int)(local - tile * a.nch);
+    const int64_t t0 = pe.off + tile * TT;
+    const int64_t tend = pe.off + pe.n;
+    const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
+    const int64_t s1 = min(s0 + pe.chunk, tend);
+
+    T xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT];
+    T vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      int64_t ti = t0 + tid + k * BLOCK;
+      ti = ti < tend ? ti : tend - 1;
+      const v4_t<T> p = a.P[ti];
+      const v4_t<T> q = a.Q[ti];
+      xt[k][0] = p.x; xt[k][1] = p.y; xt[k][2] = p.z; hst[k] = p.w;
+      at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) { vh[k][m] = 0; vl[k][m] = 0; dh[k][m] = 0; dl[k][m] = 0; }
+    }
+
+    // Stage the first tile.
+    int buf = 0;
+    if (s0 < s1) {
+      const int64_t j = s0 + tid;
+      if (j < s1) { cp_record<T>(&sP[0][tid], a.P + j); cp_record<T>(&sQ[0][tid], a.Q + j); }
+      else { sP[0][tid] = pad_P<T>(); sQ[0][tid] = pad_Q<T>(); }
+    }
+    cp_async_commit();
+
+    for (int64_t sb = s0; sb < s1; sb += TILE) {
+      const int64_t nb = sb + TILE;
+      if (nb < s1) {
+        const int64_t j = nb + tid;
+        if (j < s1) { cp_record<T>(&sP[buf ^ 1][tid], a.P + j); cp_record<T>(&sQ[buf ^ 1][tid], a.Q + j); }
+        else { sP[buf ^ 1][tid] = pad_P<T>(); sQ[buf ^ 1][tid] = pad_Q<T>(); }
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+
+#pragma unroll 1
+      for (int g = 0; g < TILE; g += CG) {
+        T sv[TPT][3], sd[TPT][3], sp[TPT][3], sdv[TPT][3], sds[TPT];
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) { sv[k][m] = 0; sd[k][m] = 0; sp[k][m] = 0; sdv[k][m] = 0; }
+          sds[k] = 0;
+        }
+#pragma unroll 4
+        for (int jj = 0; jj < CG; ++jj) {
+          const v4_t<T> p = sP[buf][g + jj];
+          const v4_t<T> q = sQ[buf][g + jj];
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
+            const T r2 = dx * dx + dy * dy + dz * dz;
+            const PairTerms<T> pt = pair_terms(r2, hst[k] + p.w);
+            // w = alpha_s x d
+            const T wx = q.y * dz - q.z * dy;
+            const T wy = q.z * dx - q.x * dz;
+            const T wz = q.x * dy - q.y * dx;
+            sv[k][0] += pt.q * wx; sv[k][1] += pt.q * wy; sv[k][2] += pt.q * wz;
+            // d . (alpha_t x alpha_s) = alpha_t . w
+            const T fd = pt.F * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
+            sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
+            sp[k][0] += pt.q * q.x; sp[k][1] += pt.q * q.y; sp[k][2] += pt.q * q.z;
+            sdv[k][0] += pt.zd * q.x; sdv[k][1] += pt.zd * q.y; sdv[k][2] += pt.zd * q.z;
+            sds[k] += pt.zd * q.w;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+          // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu (v_t sum z alpha_s - alpha_t sum z v_s)
+          const T ex = at[k][1] * sp[k][2] - at[k][2] * sp[k][1] + sd[k][0] + a.nu2 * (vt[k] * sdv[k][0] - sds[k] * at[k][0]);
+          const T ey = at[k][2] * sp[k][0] - at[k][0] * sp[k][2] + sd[k][1] + a.nu2 * (vt[k] * sdv[k][1] - sds[k] * at[k][1]);
+          const T ez = at[k][0] * sp[k][1] - at[k][1] * sp[k][0] + sd[k][2] + a.nu2 * (vt[k] * sdv[k][2] - sds[k] * at[k][2]);
+          two_sum_acc(vh[k][0], vl[k][0], sv[k][0]);
+          two_sum_acc(vh[k][1], vl[k][1], sv[k][1]);
+          two_sum_acc(vh[k][2], vl[k][2], sv[k][2]);
+          two_sum_acc(dh[k][0], dl[k][0], ex);
+          two_sum_acc(dh[k][1], dl[k][1], ey);
+          two_sum_acc(dh[k][2], dl[k][2], ez);
+        }
+      }
+      __syncthreads();
+      buf ^= 1;
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      const int64_t ti = t0 + tid + k * BLOCK;
+      if (ti < tend) {
+        double *o = a.partial + (int64_t)c * 6 * a.cap + ti;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          o[m * a.cap] = ((double)vh[k][m] + (double)vl[k][m]) * kInv4Pi;
+          o[(3 + m) * a.cap] = ((double)dh[k][m] + (double)dl[k][m]) * kInv4Pi;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- stage kernel
+struct StageArgs {
+  double *x0;          // [6][cap] FP64 state (x, y, z, ax, ay, az) at the step start
+  double *acc;         // [6][cap] RK accumulator
+  double *rates;       // [6][cap] last evaluated rates (velocity, dalpha)
+  const double *sig;   // [cap]
+  const double *vol;   // [cap]
+  const double *partial;
+  void *P;
+  void *Q;
+  const int64_t *sys_off;  // [nsys + 1] ascending slot offsets (capacity layout)
+  const int64_t *sys_n;    // [nsys]
+  int nsys;
+  int nch;
+  int64_t cap;
+  int scheme;  // 0 Euler, 1 RK3, 2 RK4, -1 rates only (solve)
+  int stage;
+  double dt;
+  double vinf[3];  // operator-split uniform inflow, applied after the final stage
+  int *flag;       // set to 1 if a non-finite value is produced
+};
+
+__device__ __forceinline__ int find_sys(const int64_t *off, int nsys, int64_t i) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T>
+__global__ void stage_kernel(StageArgs a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.cap; i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = find_sys(a.sys_off, a.nsys, i);
+    if (i - a.sys_off[s] >= a.sys_n[s]) continue;
+    double k[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      double v = 0.0;
+      for (int c = 0; c < a.nch; ++c) v += a.partial[((int64_t)c * 6 + m) * a.cap + i];
+      k[m] = v;
+      a.rates[m * a.cap + i] = v;
+    }
+    if (a.scheme < 0) continue;
+    double y[6];
+    const double dt = a.dt;
+    bool final_stage = false;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const double x = a.x0[m * a.cap + i];
+      double acc = a.acc[m * a.cap + i];
+      double yy;
+      if (a.scheme == 2) {  // classical RK4
+        if (a.stage == 0) { acc = k[m]; yy = x + 0.5 * dt * k[m]; }
+        else if (a.stage == 1) { acc += 2.0 * k[m]; yy = x + 0.5 * dt * k[m]; }
+        else if (a.stage == 2) { acc += 2.0 * k[m]; yy = x + dt * k[m]; }
+        else { yy = x + (dt / 6.0) * (acc + k[m]); final_stage = true; }
+      } else if (a.scheme == 1) {  // Kutta RK3
+        if (a.stage == 0) { acc = k[m]; yy = x + 0.5 * dt * k[m]; }
+        else if (a.stage == 1) { yy = x + dt * (2.0 * k[m] - acc); acc += 4.0 * k[m]; }
+        else { yy = x + (dt / 6.0) * (acc + k[m]); final_stage = true; }
+      } else {  // explicit Euler
+        yy = x + dt * k[m];
+        final_stage = true;
+      }
+      if (final_stage && m < 3) yy += a.vinf[m] * dt;
+      a.acc[m * a.cap + i] = acc;
+      y[m] = yy;
+    }
+    if (final_stage) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) a.x0[m * a.cap + i] = y[m];
+    }
+    bool bad = false;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) bad |= !isfinite(y[m]);
+    if (bad) *a.flag = 1;
+    const double sg = a.sig[i];
+    static_cast<v4_t<T> *>(a.P)[i] = make_v4<T>((T)y[0], (T)y[1], (T)y[2], (T)(0.5 * sg * sg));
+    static_cast<v4_t<T> *>(a.Q)[i] = make_v4<T>((T)y[3], (T)y[4], (T)y[5], (T)a.vol[i]);
+  }
+}
+
+// Pack the FP64 state at the step start into the source records.
+template <typename T>
+__global__ void pack_kernel(const double *x0, const double *sig, const double *vol, void *P, void *Q, int64_t lo,
+                            int64_t hi, int64_t cap) {
+  for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
+    const double sg = sig[i];
+    static_cast<v4_t<T> *>(P)[i] = make_v4<T>((T)x0[i], (T)x0[cap + i], (T)x0[2 * cap + i], (T)(0.5 * sg * sg));
+    static_cast<v4_t<T> *>(Q)[i] =
+        make_v4<T>((T)x0[3 * cap + i], (T)x0[4 * cap + i], (T)x0[5 * cap + i], (T)vol[i]);
+  }
+}
+
+// Host row-major (n, 3) position / strength + (n) radius / volume, staged in
+// device memory, scattered into the SoA state at slot offset `off`.
+__global__ void scatter_kernel(const double *stage, int64_t n, int64_t off, int64_t cap, double *x0, double *sig,
+                               double *vol) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      x0[m * cap + off + i] = stage[3 * i + m];
+      x0[(3 + m) * cap + off + i] = stage[3 * n + 3 * i + m];
+    }
+    sig[off + i] = stage[6 * n + i];
+    vol[off + i] = stage[7 * n + i];
+  }
+}
+
+// SoA [6][cap] (from slot offset `off`) -> row-major (n, 3) x 2.
+__global__ void gather_kernel(const double *src, int64_t n, int64_t off, int64_t cap, double *stage) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      stage[3 * i + m] = src[m * cap + off + i];
+      stage[3 * n + 3 * i + m] = src[(3 + m) * cap + off + i];
+    }
+  }
+}
+
+// Flat PAWAN state vector (per wake [x (maxN x 3) ; alpha (maxN x 3)] at offset
+// sum of 6 maxN, __interaction::setStates/getStates, interaction.cpp:337-365,
+// wake.cpp:856-893) <-> SoA state.  dir = 0: flat -> SoA, 1: SoA -> flat.
+__global__ void flat_kernel(double *flat, int64_t n, int64_t maxn, int64_t off, int64_t cap, double *soa, int dir) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      if (dir == 0) {
+        soa[m * cap + off + i] = flat[3 * i + m];
+        soa[(3 + m) * cap + off + i] = flat[3 * maxn + 3 * i + m];
+      } else {
+        flat[3 * i + m] = soa[m * cap + off + i];
+        flat[3 * maxn + 3 * i + m] = soa[(3 + m) * cap + off + i];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- diagnostics
+template <typename T> struct DiagArgs {
+  const v4_t<T> *P;
+  const v4_t<T> *Q;
+  double *partial;  // [nch][6][cap]: components 0..2 = helicity, KE, KEF row sums
+  const PlanEntry *plan;
+  int nsys;
+  int nch;
+  int64_t cap;
+  unsigned int *counters;
+};
+
+// Quadratic diagnostics: per target t and chunk, sums over sources s != t of
+//   helicity  q(rho, s_ts) (x_s - x_t).(a_t x a_s)            (HELICITY, interaction_utils.h:214-242)
+//   KE        [(rho^2 + 2 s^2) a_t.a_s + (d.a_t)(d.a_s)] / (16 pi (rho^2 + s^2)^1.5)   (:278-306)
+//   KEF       (rho^2 + 1.5 s^2) a_t.a_s / (8 pi (rho^2 + s^2)^1.5)                    (:308-331)
+// Summed over ordered pairs these equal PAWAN's 2 x sum over unordered pairs.
+template <typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
+  __shared__ __align__(16) v4_t<T> sP[BLOCK];
+  __shared__ __align__(16) v4_t<T> sQ[BLOCK];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const int64_t total = a.plan[a.nsys].item_start;
+  int64_t item;
+  while (next_item(a.counters, total, item, &s_item)) {
+    const int si = find_plan(a.plan, a.nsys, item);
+    const PlanEntry pe = a.plan[si];
+    const int64_t local = item - pe.item_start;
+    const int64_t tile = local / a.nch;
+    const int c = (int)(local - tile * a.nch);
+    const int64_t tend = pe.off + pe.n;
+    const int64_t t = min(pe.off + tile * BLOCK + tid, tend - 1);
+    const bool valid = pe.off + tile * BLOCK + tid < tend;
+    const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
+    const int64_t s1 = min(s0 + pe.chunk, tend);
+    const v4_t<T> pt = a.P[t], qt = a.Q[t];
+    double h = 0, ke = 0, kef = 0;
+    for (int64_t sb = s0; sb < s1; sb += BLOCK) {
+      __syncthreads();
+      const int64_t j = sb + tid;
+      if (j < s1) { sP[tid] = a.P[j]; sQ[tid] = a.Q[j]; }
+      else { sP[tid] = pad_P<T>(); sQ[tid] = pad_Q<T>(); }
+      __syncthreads();
+      T hh = 0, kk = 0, kf = 0;
+      const int cnt = (int)min((int64_t)BLOCK, s1 - sb);
+      for (int jj = 0; jj < cnt; ++jj) {
+        if (sb + jj == t) continue;
+        const v4_t<T> p = sP[jj], q = sQ[jj];
+        const T dx = pt.x - p.x, dy = pt.y - p.y, dz = pt.z - p.z;
+        const T r2 = dx * dx + dy * dy + dz * dz;
+        const T s2 = pt.w + p.w;
+        const PairTerms<T> k = pair_terms(r2, s2);
+        const T cx = qt.y * q.z - qt.z * q.y, cy = qt.z * q.x - qt.x * q.z, cz = qt.x * q.y - qt.y * q.x;
+        hh -= k.q * (dx * cx + dy * cy + dz * cz);
+        const T aa = qt.x * q.x + qt.y * q.y + qt.z * q.z;
+        const T dat = dx * qt.x + dy * qt.y + dz * qt.z;
+        const T das = dx * q.x + dy * q.y + dz * q.z;
+        const T rs = r2 + s2;
+        T ir;
+        if constexpr (sizeof(T) == 4) ir = fast_rsqrt(rs); else ir = rsqrt(rs);
+        const T ir3 = ir * ir * ir;
+        kk += ((r2 + T(2) * s2) * aa + dat * das) * ir3;
+        kf += (r2 + T(1.5) * s2) * aa * ir3;
+      }
+      h += (double)hh;
+      ke += (double)kk;
+      kef += (double)kf;
+    }
+    if (valid) {
+      double *o = a.partial + (int64_t)c * 6 * a.cap + t;
+      o[0] = h * kInv4Pi;
+      o[a.cap] = ke * (kInv4Pi * 0.25);      // 1/(16 pi)
+      o[2 * a.cap] = kef * (kInv4Pi * 0.5);  // 1/(8 pi)
+    }
+  }
+}
+
+// Per-wake O(N) diagnostics and the reduction of the quadratic row sums, FP64.
+// Fields (per CTA partial, summed on the host in CTA order):
+//   0-2 sum alpha, 3-5 sum x x alpha, 6-8 sum x x (x x alpha), 9 Zc numerator,
+//   10 Zc denominator, 11-13 velocity at the origin (getVi), 14 helicity,
+//   15 KE pair sum, 16 KEF pair sum, 17 KE self terms, 18 KEF self terms.
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += red[i];
+  return r;
+}
+
+__global__ void diag_wake_kernel(const double *x0, const double *sig, const double *partial, int nch, int64_t cap,
+                                 int64_t lo, int64_t hi, int quad, double *out) {
+  __shared__ double red[32];
+  double f[kDiagFields];
+#pragma unroll
+  for (int m = 0; m < kDiagFields; ++m) f[m] = 0.0;
+  for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = x0[i], y = x0[cap + i], z = x0[2 * cap + i];
+    const double ax = x0[3 * cap + i], ay = x0[4 * cap + i], az = x0[5 * cap + i];
+    f[0] += ax; f[1] += ay; f[2] += az;
+    const double cx = y * az - z * ay, cy = z * ax - x * az, cz = x * ay - y * ax;
+    f[3] += cx; f[4] += cy; f[5] += cz;
+    f[6] += y * cz - z * cy; f[7] += z * cx - x * cz; f[8] += x * cy - y * cx;
+    const double om = sqrt(ax * ax + ay * ay + az * az);
+    const double rr = x * x + y * y;
+    f[9] += om * z * rr;
+    f[10] += om * rr;
+    // getVi at the origin with the particle's own radius: d = -x
+    const double s = sig[i];
+    const double r2 = rr + z * z;
+    const PairTerms<double> k = pair_terms(r2, s * s);
+    const double q = k.q * kInv4Pi;
+    f[11] += q * (ay * (-z) - az * (-y));
+    f[12] += q * (az * (-x) - ax * (-z));
+    f[13] += q * (ax * (-y) - ay * (-x));
+    if (quad) {
+      double h = 0, ke = 0, kef = 0;
+      for (int c = 0; c < nch; ++c) {
+        h += partial[((int64_t)c * 6 + 0) * cap + i];
+        ke += partial[((int64_t)c * 6 + 1) * cap + i];
+        kef += partial[((int64_t)c * 6 + 2) * cap + i];
+      }
+      f[14] += h; f[15] += ke; f[16] += kef;
+    }
+    const double a2 = ax * ax + ay * ay + az * az;
+    f[17] += a2 / s * (kInv4Pi * 0.5);    // |a|^2 / (8 pi s)
+    f[18] += a2 / s * (kInv4Pi * 0.75);   // 3 |a|^2 / (16 pi s)
+  }
+  for (int m = 0; m < kDiagFields; ++m) {
+    const double r = block_sum(f[m], red);
+    if (threadIdx.x == 0) out[(int64_t)blockIdx.x * kDiagFields + m] = r;
+  }
+}
+
+// Velocity induced at arbitrary points by particles [lo, hi) with each
+// particle's own radius (PAWAN __interaction::getVi, interaction.cpp:453-477;
+// the blade-airstation inflow of getInflow, :399-451).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) probe_kernel(const double *x0, const double *sig, int64_t cap, int64_t lo,
+                                                      int64_t hi, const double *pts, int64_t npts, double *vel) {
+  __shared__ double sx[BLOCK][7];
+  const int64_t pi = blockIdx.x * (int64_t)BLOCK + threadIdx.x;
+  const bool valid = pi < npts;
+  const double rx = valid ? pts[3 * pi] : 0.0, ry = valid ? pts[3 * pi + 1] : 0.0, rz = valid ? pts[3 * pi + 2] : 0.0;
+  double u0 = 0, u1 = 0, u2 = 0;
+  for (int64_t sb = lo; sb < hi; sb += BLOCK) {
+    __syncthreads();
+    const int64_t j = sb + threadIdx.x;
+    if (j < hi) {
+      sx[threadIdx.x][0] = x0[j]; sx[threadIdx.x][1] = x0[cap + j]; sx[threadIdx.x][2] = x0[2 * cap + j];
+      sx[threadIdx.x][3] = x0[3 * cap + j]; sx[threadIdx.x][4] = x0[4 * cap + j]; sx[threadIdx.x][5] = x0[5 * cap + j];
+      sx[threadIdx.x][6] = sig[j];
+    }
+    __syncthreads();
+    const int cnt = (int)min((int64_t)BLOCK, hi - sb);
+    for (int jj = 0; jj < cnt; ++jj) {
+      const double dx = rx - sx[jj][0], dy = ry - sx[jj][1], dz = rz - sx[jj][2];
+      const double s = sx[jj][6];
+      const PairTerms<double> k = pair_terms(dx * dx + dy * dy + dz * dz, s * s);
+      const double q = k.q * kInv4Pi;
+      const double ax = sx[jj][3], ay = sx[jj][4], az = sx[jj][5];
+      u0 += q * (ay * dz - az * dy);
+      u1 += q * (az * dx - ax * dz);
+      u2 += q * (ax * dy - ay * dx);
+    }
+  }
+  if (valid) { vel[3 * pi] += u0; vel[3 * pi + 1] += u1; vel[3 * pi + 2] += u2; }
+}
+
+}  // namespace pgpu

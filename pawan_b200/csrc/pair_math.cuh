@@ -1,0 +1,172 @@
+// Per-pair regularised Biot-Savart / stretching / diffusion terms of PAWAN's
+// Gaussian vortex-particle kernel, for FP32 (compensated accumulation around
+// it) and FP64.
+//
+// Reference algorithm (src/interaction/gaussian.h:20-60 and
+// src/interaction/interaction_utils.h:55-105, 344-378, 523-576), per ordered
+// pair (target t, source s), d = x_t - x_s, rho = |d|,
+// sigma^2 = (sigma_s^2 + sigma_t^2)/2, u = rho^2 / sigma^2:
+//   zeta = exp(-u/2) / ((2 pi)^(3/2) sigma^3)
+//   q    = (erf(sqrt(u/2)) / (4 pi sigma^3 sqrt(u)) - zeta) / u
+//   F    = (zeta - 3 q) / rho^2
+//   u_t  += q (a_s x d)
+//   da_t += q (a_t x a_s) + F (d . (a_t x a_s)) d + nu zeta/(sigma^2/2) (v_t a_s - v_s a_t)
+//
+// Everything here is carried in units scaled by 4 pi (q' = 4 pi q, F' = 4 pi F,
+// z' = 4 pi zeta) so no per-pair constant multiplies are needed; the caller
+// multiplies the accumulated sums by 1/(4 pi) once per target.  With
+// k1 = sqrt(2/pi) = 4 pi / (2 pi)^(3/2) and r = 1/rho, s = 1/sigma:
+//   z' = k1 s^3 e^{-u/2}
+//   q' = r^2 (erf(sqrt(u/2)) r - k1 e^{-u/2} s)
+//   F' = (z' - 3 q') r^2
+//
+// Small-u branch.  The closed form cancels catastrophically as u -> 0 (q loses
+// about log10(3/u) digits, F about log10(15/u^2)).  Below a threshold the
+// series of the same functions is used instead, derived from
+//   g(x) = erf(x/sqrt2) - sqrt(2/pi) x e^{-x^2/2} = sqrt(2/pi) int_0^x t^2 e^{-t^2/2} dt
+// which gives, with u = x^2,
+//   q' = k1 s^3 S(u),   S(u) = sum_k (-1)^k u^k / (2^k k! (2k+3))
+//   F' = -k1 s^5 T(u),  T(u) = sum_m (-1)^m u^m / (2^m m! (2m+5))
+// Both are finite at u = 0, so the self pair (d = 0, a_t x a_s = 0,
+// v_t a_s - v_s a_t = 0) contributes exact zeros without an index mask.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace pgpu {
+
+// Packed particle record as stored in HBM and staged in shared memory:
+// P = (x, y, z, sigma^2/2), Q = (alpha_x, alpha_y, alpha_z, volume).
+template <typename T> struct V4;
+template <> struct V4<float> { using type = float4; };
+template <> struct V4<double> { using type = double4; };
+template <typename T> using v4_t = typename V4<T>::type;
+
+constexpr double kK1 = 0.7978845608028654;       // sqrt(2/pi)
+constexpr double kInv4Pi = 0.07957747154594767;  // 1/(4 pi)
+constexpr double kNegHalfLog2e = -0.7213475204444817;  // -0.5 / ln 2
+
+// Series coefficients S_k = (-1)^k/(2^k k!(2k+3)), T_m = (-1)^m/(2^m m!(2m+5)).
+#define PGPU_S0 0.3333333333333333
+#define PGPU_S1 -0.1
+#define PGPU_S2 0.017857142857142856
+#define PGPU_S3 -0.0023148148148148147
+#define PGPU_S4 0.00023674242424242425
+#define PGPU_S5 -2.0032051282051282e-05
+#define PGPU_S6 1.4467592592592592e-06
+#define PGPU_S7 -9.118230625583566e-08
+#define PGPU_S8 5.099010547201337e-09
+#define PGPU_T0 0.2
+#define PGPU_T1 -0.07142857142857142
+#define PGPU_T2 0.013888888888888888
+#define PGPU_T3 -0.001893939393939394
+#define PGPU_T4 0.00020032051282051281
+#define PGPU_T5 -1.736111111111111e-05
+#define PGPU_T6 1.2765522875816993e-06
+#define PGPU_T7 -8.158416875522139e-08
+#define PGPU_T8 4.613390495086924e-09
+
+// Threshold on u below which the series is used.  FP32: the closed form keeps
+// ~1e-6 relative accuracy for F at u = 1, and 9 terms of the series are
+// accurate to ~1e-8 on [0, 1].  FP64: at u = 1e-2 the closed form keeps
+// ~3e-14 and 9 terms are exact to rounding.
+template <typename T> struct SeriesCut;
+template <> struct SeriesCut<float> { static constexpr float value = 1.0f; };
+template <> struct SeriesCut<double> { static constexpr double value = 1.0e-2; };
+
+__device__ __forceinline__ float fast_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float fast_exp2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+template <typename T> struct PairTerms {
+  T q;   // 4 pi q
+  T F;   // 4 pi F
+  T zd;  // 4 pi zeta / sigma^2   (diffusion weight before the factor 2 nu)
+};
+
+// r2 = rho^2, s2 = sigma_ts^2.
+__device__ __forceinline__ PairTerms<float> pair_terms(float r2, float s2) {
+  PairTerms<float> o;
+  const float is = fast_rsqrt(s2);
+  const float is2 = is * is;
+  const float u = r2 * is2;
+  const float E = fast_exp2(u * (float)kNegHalfLog2e);
+  const float zk = (float)kK1 * is * is2;  // k1 / sigma^3
+  const float z = zk * E;
+  if (u < SeriesCut<float>::value) {
+    float S = (float)PGPU_S8;
+    S = fmaf(S, u, (float)PGPU_S7); S = fmaf(S, u, (float)PGPU_S6); S = fmaf(S, u, (float)PGPU_S5);
+    S = fmaf(S, u, (float)PGPU_S4); S = fmaf(S, u, (float)PGPU_S3); S = fmaf(S, u, (float)PGPU_S2);
+    S = fmaf(S, u, (float)PGPU_S1); S = fmaf(S, u, (float)PGPU_S0);
+    float Tt = (float)PGPU_T8;
+    Tt = fmaf(Tt, u, (float)PGPU_T7); Tt = fmaf(Tt, u, (float)PGPU_T6); Tt = fmaf(Tt, u, (float)PGPU_T5);
+    Tt = fmaf(Tt, u, (float)PGPU_T4); Tt = fmaf(Tt, u, (float)PGPU_T3); Tt = fmaf(Tt, u, (float)PGPU_T2);
+    Tt = fmaf(Tt, u, (float)PGPU_T1); Tt = fmaf(Tt, u, (float)PGPU_T0);
+    o.q = zk * S;
+    o.F = -zk * is2 * Tt;
+  } else {
+    const float ir = fast_rsqrt(r2);
+    const float ir2 = ir * ir;
+    const float y = r2 * ir * (is * 0.70710678118654752f);  // rho / (sigma sqrt 2)
+    const float er = erff(y);
+    o.q = ir2 * fmaf(-(float)kK1 * is, E, er * ir);
+    o.F = fmaf(-3.0f, o.q, z) * ir2;
+  }
+  o.zd = z * is2;
+  return o;
+}
+
+__device__ __forceinline__ PairTerms<double> pair_terms(double r2, double s2) {
+  PairTerms<double> o;
+  const double is = rsqrt(s2);
+  const double is2 = is * is;
+  const double u = r2 * is2;
+  const double E = exp(-0.5 * u);
+  const double zk = kK1 * is * is2;
+  const double z = zk * E;
+  if (u < SeriesCut<double>::value) {
+    double S = PGPU_S8;
+    S = fma(S, u, PGPU_S7); S = fma(S, u, PGPU_S6); S = fma(S, u, PGPU_S5); S = fma(S, u, PGPU_S4);
+    S = fma(S, u, PGPU_S3); S = fma(S, u, PGPU_S2); S = fma(S, u, PGPU_S1); S = fma(S, u, PGPU_S0);
+    double Tt = PGPU_T8;
+    Tt = fma(Tt, u, PGPU_T7); Tt = fma(Tt, u, PGPU_T6); Tt = fma(Tt, u, PGPU_T5); Tt = fma(Tt, u, PGPU_T4);
+    Tt = fma(Tt, u, PGPU_T3); Tt = fma(Tt, u, PGPU_T2); Tt = fma(Tt, u, PGPU_T1); Tt = fma(Tt, u, PGPU_T0);
+    o.q = zk * S;
+    o.F = -zk * is2 * Tt;
+  } else {
+    const double rho = sqrt(r2);
+    const double ir = 1.0 / rho;
+    const double ir2 = ir * ir;
+    const double er = erf(rho * is * 0.70710678118654752440);
+    o.q = ir2 * (er * ir - kK1 * is * E);
+    o.F = (z - 3.0 * o.q) * ir2;
+  }
+  o.zd = z * is2;
+  return o;
+}
+
+// Error-free addition (Knuth two-sum): hi + lo == a + b exactly.  The
+// explicit _rn intrinsics keep the compiler from contracting or reordering.
+__device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float b) {
+  const float s = __fadd_rn(hi, b);
+  const float bb = __fsub_rn(s, hi);
+  const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  hi = s;
+  lo = __fadd_rn(lo, e);
+}
+__device__ __forceinline__ void two_sum_acc(double &hi, double &lo, double b) {
+  const double s = __dadd_rn(hi, b);
+  const double bb = __dsub_rn(s, hi);
+  const double e = __dadd_rn(__dsub_rn(hi, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+  hi = s;
+  lo = __dadd_rn(lo, e);
+}
+
+}  // namespace pgpu

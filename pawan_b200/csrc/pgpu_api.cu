@@ -1,0 +1,749 @@
+// C-ABI implementation of the B200 vortex-particle backend (include/pawan_gpu.h).
+//
+// Device memory of a context (cap = total particle slots of all wakes):
+//   x0     [6][cap] FP64   state at the step start (x, y, z, alpha_x, alpha_y, alpha_z), SoA
+//   acc    [6][cap] FP64   RK accumulator
+//   rates  [6][cap] FP64   rates of the last evaluation
+//   sig, vol [cap]  FP64   smoothing radius, volume
+//   P, Q   [cap]    float4 (FP32C) or double4 (FP64) source records (x, y, z, sigma^2/2), (alpha, vol)
+//   partial [nch][6][cap] FP64 per-chunk partial rates written by the pair kernel
+//   stage  [8][cap] FP64   staging for host row-major <-> SoA transfers
+// Systems occupy contiguous slot ranges; inside a system its wakes are laid out
+// in the order they were added.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pawan_gpu.h"
+#include "kernels.cuh"
+
+using namespace pgpu;
+
+namespace {
+
+constexpr int kCG = 32;
+
+struct Shape { int block, tpt; };
+// Compiled pair-kernel shapes (the autotuner chooses among these).
+constexpr Shape kShapes[] = {{128, 1}, {128, 2}, {256, 1}, {256, 2}, {64, 2}, {128, 4}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+template <typename T> using PairFn = void (*)(PairArgs<T>);
+
+template <typename T> PairFn<T> pair_fn(int s) {
+  switch (s) {
+    case 0: return pair_kernel<T, 128, 1, kCG>;
+    case 1: return pair_kernel<T, 128, 2, kCG>;
+    case 2: return pair_kernel<T, 256, 1, kCG>;
+    case 3: return pair_kernel<T, 256, 2, kCG>;
+    case 4: return pair_kernel<T, 64, 2, kCG>;
+    default: return pair_kernel<T, 128, 4, kCG>;
+  }
+}
+
+struct WakeRec {
+  int sys;
+  int64_t cap, n, off;
+};
+struct SysRec {
+  std::vector<int> wakes;
+  int64_t off = 0, cap = 0;
+  double zc = 0.0;  // last reported Zc (PAWAN keeps _Zc across calls)
+};
+
+}  // namespace
+
+struct pgpu_ctx {
+  pgpu_config cfg;
+  cudaStream_t st = nullptr;
+  int sms = 0;
+  std::vector<WakeRec> wakes;
+  std::vector<SysRec> sys;
+  bool frozen = false;
+  int64_t cap = 0;
+  double *x0 = nullptr, *acc = nullptr, *rates = nullptr, *sig = nullptr, *vol = nullptr;
+  double *partial = nullptr, *stage = nullptr, *d_diag = nullptr;
+  void *P = nullptr, *Q = nullptr;
+  int64_t *d_sysoff = nullptr, *d_sysn = nullptr;
+  PlanEntry *d_plan = nullptr, *d_plan_diag = nullptr;
+  unsigned int *d_counters = nullptr;
+  int *d_flag = nullptr;
+  int diag_blocks = 0;
+  int shape = 3;
+  int grid[kNumShapes] = {0};
+  int nch = 1;
+  bool plan_dirty = true;
+  bool timing = true;
+  cudaEvent_t ev[8][2];
+  double pair_ms = 0.0;
+  int64_t pair_launches = 0;
+  int64_t launches = 0;
+  std::map<std::tuple<int, double, int, int>, cudaGraphExec_t> graphs;
+  std::vector<cudaGraph_t> graph_defs;
+  std::string err;
+};
+
+namespace {
+
+int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                    \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess) return fail(c, PGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+bool fp64(const pgpu_ctx *c) { return c->cfg.precision == PGPU_FP64; }
+size_t rec_bytes(const pgpu_ctx *c) { return fp64(c) ? sizeof(double4) : sizeof(float4); }
+
+int64_t sys_n(const pgpu_ctx *c, int s) {
+  const SysRec &S = c->sys[s];
+  if (S.wakes.empty()) return 0;
+  const WakeRec &L = c->wakes[S.wakes.back()];
+  return (L.off - S.off) + L.n;
+}
+
+int check_contiguous(pgpu_ctx *c) {
+  for (size_t s = 0; s < c->sys.size(); ++s) {
+    const SysRec &S = c->sys[s];
+    for (size_t k = 0; k + 1 < S.wakes.size(); ++k) {
+      const WakeRec &W = c->wakes[S.wakes[k]];
+      if (W.n != W.cap)
+        return fail(c, PGPU_EINVAL,
+                    "wake %d of system %zu holds %lld of %lld particles; every wake but the last of a system must be full",
+                    S.wakes[k], s, (long long)W.n, (long long)W.cap);
+    }
+  }
+  return PGPU_OK;
+}
+
+template <typename T> int occupancy(pgpu_ctx *c, int s) {
+  int nb = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pair_fn<T>(s), kShapes[s].block, 0);
+  if (e != cudaSuccess || nb < 1) nb = 1;
+  return nb * c->sms;
+}
+
+// Freeze the slot layout and allocate device memory (first upload).
+int freeze(pgpu_ctx *c) {
+  if (c->frozen) return PGPU_OK;
+  if (c->wakes.empty()) return fail(c, PGPU_EINVAL, "no wakes were added");
+  int64_t off = 0;
+  for (auto &S : c->sys) {
+    S.off = off;
+    for (int w : S.wakes) {
+      c->wakes[w].off = off;
+      off += c->wakes[w].cap;
+    }
+    S.cap = off - S.off;
+  }
+  c->cap = std::max<int64_t>(off, 1);
+  const int64_t cap = c->cap;
+  auto alloc = [&](void **p, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return fail(c, PGPU_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    return PGPU_OK;
+  };
+  int r;
+  if ((r = alloc((void **)&c->x0, 6 * cap * sizeof(double)))) return r;
+  if ((r = alloc((void **)&c->acc, 6 * cap * sizeof(double)))) return r;
+  if ((r = alloc((void **)&c->rates, 6 * cap * sizeof(double)))) return r;
+  if ((r = alloc((void **)&c->sig, cap * sizeof(double)))) return r;
+  if ((r = alloc((void **)&c->vol, cap * sizeof(double)))) return r;
+  if ((r = alloc((void **)&c->stage, 8 * cap * sizeof(double)))) return r;
+  if ((r = alloc((void **)&c->partial, (size_t)kMaxChunks * 6 * cap * sizeof(double)))) return r;
+  if ((r = alloc(&c->P, cap * rec_bytes(c)))) return r;
+  if ((r = alloc(&c->Q, cap * rec_bytes(c)))) return r;
+  const size_t ns = c->sys.size();
+  if ((r = alloc((void **)&c->d_sysoff, (ns + 1) * sizeof(int64_t)))) return r;
+  if ((r = alloc((void **)&c->d_sysn, ns * sizeof(int64_t)))) return r;
+  if ((r = alloc((void **)&c->d_plan, (ns + 1) * sizeof(PlanEntry)))) return r;
+  if ((r = alloc((void **)&c->d_plan_diag, 2 * sizeof(PlanEntry)))) return r;
+  if ((r = alloc((void **)&c->d_counters, 4 * sizeof(unsigned int)))) return r;
+  if ((r = alloc((void **)&c->d_flag, sizeof(int)))) return r;
+  c->diag_blocks = 2 * c->sms;
+  if ((r = alloc((void **)&c->d_diag, (size_t)c->diag_blocks * kDiagFields * sizeof(double)))) return r;
+  CK(cudaMemsetAsync(c->x0, 0, 6 * cap * sizeof(double), c->st));
+  CK(cudaMemsetAsync(c->acc, 0, 6 * cap * sizeof(double), c->st));
+  CK(cudaMemsetAsync(c->rates, 0, 6 * cap * sizeof(double), c->st));
+  CK(cudaMemsetAsync(c->sig, 0, cap * sizeof(double), c->st));
+  CK(cudaMemsetAsync(c->vol, 0, cap * sizeof(double), c->st));
+  CK(cudaMemsetAsync(c->partial, 0, (size_t)kMaxChunks * 6 * cap * sizeof(double), c->st));
+  CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned int), c->st));
+  CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->st));
+  for (int s = 0; s < kNumShapes; ++s) c->grid[s] = fp64(c) ? occupancy<double>(c, s) : occupancy<float>(c, s);
+  c->frozen = true;
+  c->plan_dirty = true;
+  return PGPU_OK;
+}
+
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Work list: systems by decreasing size, target tiles x source chunks each.
+std::vector<PlanEntry> build_plan(const pgpu_ctx *c, const std::vector<int> &systems, int shape, int nch) {
+  const int64_t TT = (int64_t)kShapes[shape].block * kShapes[shape].tpt;
+  const int64_t TILE = kShapes[shape].block;
+  std::vector<std::pair<int64_t, int>> order;
+  for (int s : systems) order.push_back({sys_n(c, s), s});
+  std::stable_sort(order.begin(), order.end(), [](auto &a, auto &b) { return a.first > b.first; });
+  std::vector<PlanEntry> plan;
+  int64_t item = 0;
+  for (auto &o : order) {
+    const int64_t n = o.first;
+    if (n <= 0) continue;
+    PlanEntry e;
+    e.off = c->sys[o.second].off;
+    e.n = n;
+    e.item_start = item;
+    e.tiles = ceil_div(n, TT);
+    e.chunk = ceil_div(ceil_div(n, nch), TILE) * TILE;
+    item += e.tiles * nch;
+    plan.push_back(e);
+  }
+  PlanEntry sentinel{};
+  sentinel.item_start = item;
+  plan.push_back(sentinel);
+  return plan;
+}
+
+int choose_nch(const pgpu_ctx *c, int shape) {
+  if (c->cfg.chunks > 0) return std::min(c->cfg.chunks, kMaxChunks);
+  const int64_t TT = (int64_t)kShapes[shape].block * kShapes[shape].tpt;
+  int64_t tiles = 0;
+  for (size_t s = 0; s < c->sys.size(); ++s) tiles += ceil_div(sys_n(c, (int)s), TT);
+  if (tiles <= 0) return 1;
+  const int64_t want = 24LL * c->grid[shape];
+  return (int)std::max<int64_t>(1, std::min<int64_t>(kMaxChunks, ceil_div(want, tiles)));
+}
+
+int upload_plan(pgpu_ctx *c) {
+  if (!c->plan_dirty) return PGPU_OK;
+  int r = check_contiguous(c);
+  if (r) return r;
+  c->nch = choose_nch(c, c->shape);
+  std::vector<int> all(c->sys.size());
+  for (size_t s = 0; s < all.size(); ++s) all[s] = (int)s;
+  std::vector<PlanEntry> plan = build_plan(c, all, c->shape, c->nch);
+  // Unused tail entries keep the sentinel item_start so the device search is bounded.
+  plan.resize(c->sys.size() + 1, plan.back());
+  std::vector<int64_t> off(c->sys.size() + 1), n(c->sys.size());
+  for (size_t s = 0; s < c->sys.size(); ++s) { off[s] = c->sys[s].off; n[s] = sys_n(c, (int)s); }
+  off[c->sys.size()] = c->cap;
+  CK(cudaMemcpyAsync(c->d_plan, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_sysoff, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_sysn, n.data(), n.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->st));
+  // Pageable host sources: make sure the copies are done before the vectors go away.
+  CK(cudaStreamSynchronize(c->st));
+  c->plan_dirty = false;
+  return PGPU_OK;
+}
+
+template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
+  PairArgs<T> a;
+  a.P = static_cast<const v4_t<T> *>(c->P);
+  a.Q = static_cast<const v4_t<T> *>(c->Q);
+  a.partial = c->partial;
+  a.plan = c->d_plan;
+  a.nsys = (int)c->sys.size();
+  a.nch = c->nch;
+  a.cap = c->cap;
+  a.nu2 = (T)(2.0 * c->cfg.nu);
+  a.counters = c->d_counters;
+  if (c->timing && slot >= 0) CK(cudaEventRecord(c->ev[slot][0], c->st));
+  pair_fn<T>(c->shape)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
+  CK(cudaGetLastError());
+  if (c->timing && slot >= 0) CK(cudaEventRecord(c->ev[slot][1], c->st));
+  c->launches++;
+  return PGPU_OK;
+}
+
+int launch_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
+  StageArgs s;
+  s.x0 = c->x0; s.acc = c->acc; s.rates = c->rates; s.sig = c->sig; s.vol = c->vol;
+  s.partial = c->partial; s.P = c->P; s.Q = c->Q;
+  s.sys_off = c->d_sysoff; s.sys_n = c->d_sysn; s.nsys = (int)c->sys.size();
+  s.nch = c->nch; s.cap = c->cap; s.scheme = scheme; s.stage = stage; s.dt = dt;
+  for (int m = 0; m < 3; ++m) s.vinf[m] = c->cfg.vinf[m];
+  s.flag = c->d_flag;
+  const int block = 256;
+  const int grid = (int)std::min<int64_t>(ceil_div(c->cap, block), 16LL * c->sms);
+  if (fp64(c)) stage_kernel<double><<<grid, block, 0, c->st>>>(s);
+  else stage_kernel<float><<<grid, block, 0, c->st>>>(s);
+  CK(cudaGetLastError());
+  c->launches++;
+  return PGPU_OK;
+}
+
+int launch_pack(pgpu_ctx *c, int64_t lo, int64_t hi) {
+  if (hi <= lo) return PGPU_OK;
+  const int block = 256;
+  const int grid = (int)std::min<int64_t>(ceil_div(hi - lo, block), 16LL * c->sms);
+  if (fp64(c)) pack_kernel<double><<<grid, block, 0, c->st>>>(c->x0, c->sig, c->vol, c->P, c->Q, lo, hi, c->cap);
+  else pack_kernel<float><<<grid, block, 0, c->st>>>(c->x0, c->sig, c->vol, c->P, c->Q, lo, hi, c->cap);
+  CK(cudaGetLastError());
+  c->launches++;
+  return PGPU_OK;
+}
+
+int launch_eval(pgpu_ctx *c, int slot) {
+  return fp64(c) ? launch_pair<double>(c, slot) : launch_pair<float>(c, slot);
+}
+
+int collect_timing(pgpu_ctx *c, int nslots) {
+  if (!c->timing) return PGPU_OK;
+  for (int k = 0; k < nslots; ++k) {
+    CK(cudaEventSynchronize(c->ev[k][1]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[k][0], c->ev[k][1]));
+    c->pair_ms += ms;
+    c->pair_launches++;
+  }
+  return PGPU_OK;
+}
+
+int stages_of(int scheme) { return scheme == PGPU_RK4 ? 4 : scheme == PGPU_RK3 ? 3 : 1; }
+
+int record_step(pgpu_ctx *c, int scheme, double dt) {
+  const int ns = stages_of(scheme);
+  for (int k = 0; k < ns; ++k) {
+    int r = launch_eval(c, k);
+    if (r) return r;
+    if ((r = launch_stage(c, scheme, k, dt))) return r;
+  }
+  return PGPU_OK;
+}
+
+int wake_ok(pgpu_ctx *c, int32_t wake) {
+  if (!c) return PGPU_EINVAL;
+  if (wake < 0 || wake >= (int32_t)c->wakes.size()) return fail(c, PGPU_EINVAL, "invalid wake id %d", wake);
+  return PGPU_OK;
+}
+
+int upload_rows(pgpu_ctx *c, const WakeRec &W, int64_t first, int64_t m, const double *pos, const double *alpha,
+                const double *sigma, const double *vol) {
+  if (m <= 0) return PGPU_OK;
+  if (!pos || !alpha || !sigma || !vol) return fail(c, PGPU_EINVAL, "null particle array");
+  CK(cudaMemcpyAsync(c->stage, pos, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->stage + 3 * m, alpha, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->stage + 6 * m, sigma, m * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->stage + 7 * m, vol, m * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  const int grid = (int)std::min<int64_t>(ceil_div(m, 256), 16LL * c->sms);
+  scatter_kernel<<<grid, 256, 0, c->st>>>(c->stage, m, W.off + first, c->cap, c->x0, c->sig, c->vol);
+  CK(cudaGetLastError());
+  c->launches++;
+  return launch_pack(c, W.off + first, W.off + first + m);
+}
+
+}  // namespace
+
+extern "C" {
+
+void pgpu_config_default(pgpu_config *cfg) {
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->precision = PGPU_FP32C;
+  cfg->device = 0;
+  cfg->nu = 1.56e-5;
+  cfg->use_graphs = 1;
+}
+
+const char *pgpu_version(void) { return "pawan_b200 0.1 (sm_100a)"; }
+
+int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
+  if (!out) return PGPU_EINVAL;
+  *out = nullptr;
+  pgpu_ctx *c = new pgpu_ctx;
+  if (cfg) c->cfg = *cfg;
+  else pgpu_config_default(&c->cfg);
+  if (c->cfg.precision != PGPU_FP32C && c->cfg.precision != PGPU_FP64) {
+    delete c;
+    return PGPU_EINVAL;
+  }
+  cudaError_t e = cudaSetDevice(c->cfg.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device);
+  for (int k = 0; k < 8 && e == cudaSuccess; ++k) {
+    e = cudaEventCreate(&c->ev[k][0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev[k][1]);
+  }
+  if (e != cudaSuccess) {
+    delete c;
+    return PGPU_ECUDA;
+  }
+  if (c->cfg.block > 0 || c->cfg.tpt > 0) {
+    int found = -1;
+    for (int s = 0; s < kNumShapes; ++s)
+      if ((c->cfg.block <= 0 || kShapes[s].block == c->cfg.block) && (c->cfg.tpt <= 0 || kShapes[s].tpt == c->cfg.tpt)) {
+        found = s;
+        break;
+      }
+    if (found < 0) {
+      cudaStreamDestroy(c->st);
+      delete c;
+      return PGPU_EINVAL;
+    }
+    c->shape = found;
+  }
+  *out = c;
+  return PGPU_OK;
+}
+
+int pgpu_destroy(pgpu_ctx *c) {
+  if (!c) return PGPU_EINVAL;
+  cudaStreamSynchronize(c->st);
+  for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
+  for (auto g : c->graph_defs) cudaGraphDestroy(g);
+  void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
+                  c->d_sysoff, c->d_sysn, c->d_plan, c->d_plan_diag, c->d_counters, c->d_flag};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
+  cudaStreamDestroy(c->st);
+  delete c;
+  return PGPU_OK;
+}
+
+int pgpu_add_wake(pgpu_ctx *c, int32_t system, int64_t capacity, int32_t *wake_id) {
+  if (!c) return PGPU_EINVAL;
+  if (c->frozen) return fail(c, PGPU_EINVAL, "wakes must be added before the first particle upload");
+  if (system < 0 || system > 1 << 20) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
+  if (capacity < 0 || capacity > (int64_t)1 << 31) return fail(c, PGPU_EINVAL, "invalid capacity %lld", (long long)capacity);
+  if ((int)c->sys.size() <= system) c->sys.resize(system + 1);
+  WakeRec w{system, capacity, 0, 0};
+  c->wakes.push_back(w);
+  c->sys[system].wakes.push_back((int)c->wakes.size() - 1);
+  if (wake_id) *wake_id = (int32_t)c->wakes.size() - 1;
+  return PGPU_OK;
+}
+
+int pgpu_set_particles(pgpu_ctx *c, int32_t wake, int64_t n, const double *pos, const double *alpha,
+                       const double *sigma, const double *vol) {
+  int r = wake_ok(c, wake);
+  if (r) return r;
+  if ((r = freeze(c))) return r;
+  WakeRec &W = c->wakes[wake];
+  if (n < 0 || n > W.cap) return fail(c, PGPU_EINVAL, "n=%lld exceeds the capacity %lld of wake %d", (long long)n, (long long)W.cap, wake);
+  if ((r = upload_rows(c, W, 0, n, pos, alpha, sigma, vol))) return r;
+  W.n = n;
+  c->plan_dirty = true;
+  return PGPU_OK;
+}
+
+int pgpu_append_particles(pgpu_ctx *c, int32_t wake, int64_t m, const double *pos, const double *alpha,
+                          const double *sigma, const double *vol) {
+  int r = wake_ok(c, wake);
+  if (r) return r;
+  if ((r = freeze(c))) return r;
+  WakeRec &W = c->wakes[wake];
+  if (c->sys[W.sys].wakes.back() != wake) return fail(c, PGPU_EINVAL, "only the last wake of a system can grow");
+  if (m < 0 || W.n + m > W.cap) return fail(c, PGPU_EINVAL, "appending %lld particles exceeds the capacity of wake %d", (long long)m, wake);
+  if ((r = upload_rows(c, W, W.n, m, pos, alpha, sigma, vol))) return r;
+  // Appended particles start a step with a zero RK accumulator.
+  W.n += m;
+  c->plan_dirty = true;
+  return PGPU_OK;
+}
+
+int pgpu_get_num_particles(pgpu_ctx *c, int32_t wake, int64_t *n) {
+  int r = wake_ok(c, wake);
+  if (r) return r;
+  if (n) *n = c->wakes[wake].n;
+  return PGPU_OK;
+}
+
+static int download_rows(pgpu_ctx *c, const double *src, const WakeRec &W, double *a, double *b) {
+  if (W.n == 0) return PGPU_OK;
+  const int grid = (int)std::min<int64_t>(ceil_div(W.n, 256), 16LL * c->sms);
+  gather_kernel<<<grid, 256, 0, c->st>>>(src, W.n, W.off, c->cap, c->stage);
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(a, c->stage, 3 * W.n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(b, c->stage + 3 * W.n, 3 * W.n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return PGPU_OK;
+}
+
+int pgpu_get_state(pgpu_ctx *c, int32_t wake, double *pos, double *alpha) {
+  int r = wake_ok(c, wake);
+  if (r) return r;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (!pos || !alpha) return fail(c, PGPU_EINVAL, "null output array");
+  return download_rows(c, c->x0, c->wakes[wake], pos, alpha);
+}
+
+int pgpu_get_rates(pgpu_ctx *c, int32_t wake, double *vel, double *dalpha) {
+  int r = wake_ok(c, wake);
+  if (r) return r;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (!vel || !dalpha) return fail(c, PGPU_EINVAL, "null output array");
+  return download_rows(c, c->rates, c->wakes[wake], vel, dalpha);
+}
+
+static int flat_io(pgpu_ctx *c, double *flat, const int64_t *maxn, int32_t nwakes, int dir, const double *soa_src) {
+  if (!c) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (!flat || !maxn || nwakes != (int32_t)c->wakes.size()) return fail(c, PGPU_EINVAL, "flat state needs one capacity per wake");
+  int64_t off = 0;
+  for (int w = 0; w < nwakes; ++w) {
+    const WakeRec &W = c->wakes[w];
+    if (maxn[w] < W.n) return fail(c, PGPU_EINVAL, "maxn[%d] is smaller than the wake size", w);
+    const int64_t sz = 6 * maxn[w];
+    if (W.n > 0) {
+      const int grid = (int)std::min<int64_t>(ceil_div(W.n, 256), 16LL * c->sms);
+      if (dir == 0) {
+        CK(cudaMemcpyAsync(c->stage, flat + off, 3 * W.n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->stage + 3 * W.n, flat + off + 3 * maxn[w], 3 * W.n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        flat_kernel<<<grid, 256, 0, c->st>>>(c->stage, W.n, W.n, W.off, c->cap, c->x0, 0);
+        CK(cudaGetLastError());
+        c->launches++;
+        int r = launch_pack(c, W.off, W.off + W.n);
+        if (r) return r;
+        CK(cudaStreamSynchronize(c->st));
+      } else {
+        flat_kernel<<<grid, 256, 0, c->st>>>(c->stage, W.n, W.n, W.off, c->cap, const_cast<double *>(soa_src), 1);
+        CK(cudaGetLastError());
+        c->launches++;
+        CK(cudaMemcpyAsync(flat + off, c->stage, 3 * W.n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaMemcpyAsync(flat + off + 3 * maxn[w], c->stage + 3 * W.n, 3 * W.n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+      }
+    }
+    off += sz;
+  }
+  return PGPU_OK;
+}
+
+int pgpu_set_states_flat(pgpu_ctx *c, const double *state, const int64_t *maxn, int32_t nwakes) {
+  return flat_io(c, const_cast<double *>(state), maxn, nwakes, 0, nullptr);
+}
+int pgpu_get_states_flat(pgpu_ctx *c, double *state, const int64_t *maxn, int32_t nwakes) {
+  return flat_io(c, state, maxn, nwakes, 1, c ? c->x0 : nullptr);
+}
+int pgpu_get_rates_flat(pgpu_ctx *c, double *rate, const int64_t *maxn, int32_t nwakes) {
+  return flat_io(c, rate, maxn, nwakes, 1, c ? c->rates : nullptr);
+}
+
+int pgpu_solve(pgpu_ctx *c) {
+  if (!c) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  int r = upload_plan(c);
+  if (r) return r;
+  if ((r = launch_eval(c, 0))) return r;
+  if ((r = launch_stage(c, -1, 0, 0.0))) return r;
+  return collect_timing(c, 1);
+}
+
+int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
+  if (!c) return PGPU_EINVAL;
+  if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
+  if (nsteps < 0) return fail(c, PGPU_EINVAL, "negative step count");
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  int r = upload_plan(c);
+  if (r) return r;
+  const int ns = stages_of(scheme);
+  if (!c->cfg.use_graphs) {
+    for (int i = 0; i < nsteps; ++i) {
+      if ((r = record_step(c, scheme, dt))) return r;
+      if ((r = collect_timing(c, ns))) return r;
+    }
+    return PGPU_OK;
+  }
+  auto key = std::make_tuple(scheme, dt, c->shape, c->nch);
+  auto it = c->graphs.find(key);
+  if (it == c->graphs.end()) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = c->launches;
+    r = record_step(c, scheme, dt);
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(c, PGPU_ECUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    c->launches = before;  // counted at replay
+    cudaGraphExec_t ex;
+    CK(cudaGraphInstantiate(&ex, g, 0));
+    c->graph_defs.push_back(g);
+    it = c->graphs.emplace(key, ex).first;
+  }
+  for (int i = 0; i < nsteps; ++i) {
+    CK(cudaGraphLaunch(it->second, c->st));
+    c->launches += 2 * ns;
+    if ((r = collect_timing(c, ns))) return r;
+  }
+  return PGPU_OK;
+}
+
+int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
+  if (!c || !out) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
+  int r = check_contiguous(c);
+  if (r) return r;
+  const int shape = 2;  // 256-thread tiles for the diagnostic pair sums
+  const int block = 256;
+  const int nch = std::max(1, std::min(kMaxChunks, (int)ceil_div(8LL * c->sms, std::max<int64_t>(1, ceil_div(sys_n(c, system), block)))));
+  std::vector<PlanEntry> plan = build_plan(c, {system}, shape, nch);
+  CK(cudaMemcpyAsync(c->d_plan_diag, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const bool quad = plan.size() > 1;
+  if (quad) {
+    int grid = 0;
+    if (fp64(c)) {
+      DiagArgs<double> a{static_cast<const double4 *>(c->P), static_cast<const double4 *>(c->Q), c->partial,
+                         c->d_plan_diag, 1, nch, c->cap, c->d_counters};
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, diag_pair_kernel<double, 256>, block, 0);
+      diag_pair_kernel<double, 256><<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
+    } else {
+      DiagArgs<float> a{static_cast<const float4 *>(c->P), static_cast<const float4 *>(c->Q), c->partial,
+                        c->d_plan_diag, 1, nch, c->cap, c->d_counters};
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, diag_pair_kernel<float, 256>, block, 0);
+      diag_pair_kernel<float, 256><<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
+    }
+    CK(cudaGetLastError());
+    c->launches++;
+  }
+  double f[kDiagFields] = {0};
+  double zc = c->sys[system].zc;
+  std::vector<double> h((size_t)c->diag_blocks * kDiagFields);
+  for (int w : c->sys[system].wakes) {
+    const WakeRec &W = c->wakes[w];
+    if (W.n == 0) continue;
+    const int grid = (int)std::min<int64_t>(ceil_div(W.n, 256), c->diag_blocks);
+    diag_wake_kernel<<<grid, 256, 0, c->st>>>(c->x0, c->sig, c->partial, nch, c->cap, W.off, W.off + W.n, quad ? 1 : 0, c->d_diag);
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemcpyAsync(h.data(), c->d_diag, (size_t)grid * kDiagFields * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    double g[kDiagFields] = {0};
+    for (int b = 0; b < grid; ++b)
+      for (int m = 0; m < kDiagFields; ++m) g[m] += h[(size_t)b * kDiagFields + m];
+    for (int m = 0; m < kDiagFields; ++m) f[m] += g[m];
+    if (g[10] != 0.0) zc = g[9] / g[10];
+  }
+  c->sys[system].zc = zc;
+  for (int m = 0; m < 3; ++m) {
+    out[m] = f[m];
+    out[3 + m] = 0.5 * f[3 + m];
+    out[6 + m] = f[6 + m] / 3.0;
+  }
+  out[9] = f[14];
+  out[10] = 0.0;
+  out[11] = 0.0;
+  out[12] = f[17] + f[15];
+  out[13] = f[18] + f[16];
+  out[14] = zc;
+  if (vbi)
+    for (int m = 0; m < 3; ++m) vbi[m] = f[11 + m];
+  return PGPU_OK;
+}
+
+int pgpu_probe(pgpu_ctx *c, int32_t system, int64_t npts, const double *pts, double *vel) {
+  if (!c) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
+  if (npts < 0 || (npts > 0 && (!pts || !vel))) return fail(c, PGPU_EINVAL, "bad probe arrays");
+  if (npts == 0) return PGPU_OK;
+  double *d = nullptr;
+  CK(cudaMallocAsync((void **)&d, 6 * npts * sizeof(double), c->st));
+  CK(cudaMemcpyAsync(d, pts, 3 * npts * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(d + 3 * npts, 0, 3 * npts * sizeof(double), c->st));
+  const int64_t lo = c->sys[system].off, hi = lo + sys_n(c, system);
+  if (hi > lo) {
+    probe_kernel<128><<<(unsigned)ceil_div(npts, 128), 128, 0, c->st>>>(c->x0, c->sig, c->cap, lo, hi, d, npts, d + 3 * npts);
+    CK(cudaGetLastError());
+    c->launches++;
+  }
+  CK(cudaMemcpyAsync(vel, d + 3 * npts, 3 * npts * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(d, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return PGPU_OK;
+}
+
+int pgpu_sync(pgpu_ctx *c) {
+  if (!c) return PGPU_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  if (c->frozen) {
+    int flag = 0;
+    CK(cudaMemcpy(&flag, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      CK(cudaMemset(c->d_flag, 0, sizeof(int)));
+      return fail(c, PGPU_ENUMERIC, "a time step produced a non-finite particle state");
+    }
+  }
+  return PGPU_OK;
+}
+
+int pgpu_pair_kernel_time(pgpu_ctx *c, double *ms, int64_t *launches) {
+  if (!c) return PGPU_EINVAL;
+  if (ms) *ms = c->pair_ms;
+  if (launches) *launches = c->pair_launches;
+  c->pair_ms = 0.0;
+  c->pair_launches = 0;
+  return PGPU_OK;
+}
+
+int64_t pgpu_launch_count(pgpu_ctx *c) { return c ? c->launches : -1; }
+
+int pgpu_kernel_shapes(int *block, int *tpt, int max) {
+  for (int s = 0; s < kNumShapes && s < max; ++s) {
+    if (block) block[s] = kShapes[s].block;
+    if (tpt) tpt[s] = kShapes[s].tpt;
+  }
+  return kNumShapes;
+}
+
+int pgpu_autotune(pgpu_ctx *c, int reps, int *block, int *tpt, double *ms_per_launch) {
+  if (!c) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (reps < 1) reps = 1;
+  const int saved = c->shape;
+  double best = 1e300;
+  int best_s = saved;
+  double ms_acc;
+  int64_t nl;
+  int r = pgpu_pair_kernel_time(c, &ms_acc, &nl);  // reset counters
+  for (int s = 0; s < kNumShapes; ++s) {
+    c->shape = s;
+    c->plan_dirty = true;
+    if ((r = upload_plan(c))) return r;
+    if ((r = launch_eval(c, 0))) return r;  // warm-up
+    if ((r = collect_timing(c, 1))) return r;
+    pgpu_pair_kernel_time(c, nullptr, nullptr);
+    for (int k = 0; k < reps; ++k) {
+      if ((r = launch_eval(c, 0))) return r;
+      if ((r = collect_timing(c, 1))) return r;
+    }
+    double ms;
+    pgpu_pair_kernel_time(c, &ms, &nl);
+    ms /= reps;
+    if (ms_per_launch) ms_per_launch[s] = ms;
+    if (ms < best) { best = ms; best_s = s; }
+  }
+  c->shape = best_s;
+  c->plan_dirty = true;
+  if ((r = upload_plan(c))) return r;
+  // The partial buffer now holds the last candidate's chunks: recompute the
+  // rates of the current state with the chosen shape.
+  if ((r = pgpu_solve(c))) return r;
+  pgpu_pair_kernel_time(c, nullptr, nullptr);
+  if (block) *block = kShapes[best_s].block;
+  if (tpt) *tpt = kShapes[best_s].tpt;
+  return PGPU_OK;
+}
+
+const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+}  // extern "C"

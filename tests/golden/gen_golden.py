@@ -1,0 +1,106 @@
+"""Generates the golden fixtures under tests/golden/ from PAWAN's own code.
+
+    make -C oracle && python tests/golden/gen_golden.py
+
+Every output comes from ``oracle/_ref/libpawanref.so``: PAWAN's unmodified
+interaction / parallel / integration / wake sources compiled against the
+project's GSL-subset shim (``oracle/Makefile``).  Inputs come from the seeded
+generators in ``pawan_b200.cases``; their SHA-256 is stored so a test can
+check that regenerating the inputs reproduces the fixture's inputs.
+
+Fixtures:
+  ring1000.npz   - 40-station ring (N=1000, sigma=0.1, nu=1e-4): inputs, rates
+                   of one solve, diagnostics and vbi, state after 2 RK4 steps
+                   and after 2 RK3 steps (dt=0.01).
+  ring5000.npz   - the 5000-particle ring (200 stations x 25, seed 0): rates on
+                   256 sampled rows, diagnostics, and the sampled rows of the
+                   state after one RK4 step (dt=0.01).
+  twowake.npz    - two interacting wakes in one system (leapfrog pair, N=400+320).
+  integrate/     - the .wake / .diagnosis files of PAWAN's own
+                   __integration::integrate for 3 RK4 steps of ring1000.
+"""
+from __future__ import annotations
+
+import hashlib
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import oracle as O  # noqa: E402
+from pawan_b200 import cases  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+NU = 1e-4
+
+
+def digest(w) -> str:
+    h = hashlib.sha256()
+    for a in (w.pos, w.alpha, w.sigma, w.vol):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def ring1000():
+    w = cases.ring_stations(stations=40, seed=0)
+    R = O.RefSystem([w], NU)
+    R.solve()
+    vel, da = R.rates()
+    diag = R.diagnose()
+    vbi = R.getvi([0.0, 0.0, 0.0])
+    R.step("rk4", 0.01, 2)
+    x4, a4 = R.state()
+    R3 = O.RefSystem([w], NU)
+    R3.step("rk3", 0.01, 2)
+    x3, a3 = R3.state()
+    np.savez_compressed(OUT / "ring1000.npz", pos=w.pos, alpha=w.alpha, sigma=w.sigma, vol=w.vol, nu=NU,
+                        vel=vel, dalpha=da, diag=diag, vbi=vbi, rk4_pos=x4, rk4_alpha=a4, rk3_pos=x3,
+                        rk3_alpha=a3, dt=0.01, sha256=digest(w))
+
+
+def ring5000():
+    w = cases.ring_stations()
+    rows = np.sort(np.random.default_rng(123).choice(w.n, 256, replace=False))
+    R = O.RefSystem([w], NU)
+    R.solve()
+    vel, da = R.rates()
+    diag = R.diagnose()
+    vbi = R.getvi([0.0, 0.0, 0.0])
+    R.step("rk4", 0.01, 1)
+    x4, a4 = R.state()
+    np.savez_compressed(OUT / "ring5000.npz", rows=rows, vel=vel[rows], dalpha=da[rows], diag=diag, vbi=vbi,
+                        rk4_pos=x4[rows], rk4_alpha=a4[rows], dt=0.01, nu=NU, sha256=digest(w))
+
+
+def twowake():
+    w1 = cases.ring_stations(stations=16, seed=3)
+    w2 = cases.ring_stations(R=1.2, stations=16, z0=0.3, seed=5).subset(320)
+    R = O.RefSystem([w1, w2], NU)
+    R.solve()
+    v1, d1 = R.rates(0)
+    v2, d2 = R.rates(1)
+    diag = R.diagnose()
+    np.savez_compressed(OUT / "twowake.npz", pos1=w1.pos, alpha1=w1.alpha, sigma1=w1.sigma, vol1=w1.vol,
+                        pos2=w2.pos, alpha2=w2.alpha, sigma2=w2.sigma, vol2=w2.vol, vel1=v1, dalpha1=d1,
+                        vel2=v2, dalpha2=d2, diag=diag, nu=NU)
+
+
+def integrate_files():
+    d = OUT / "integrate"
+    d.mkdir(exist_ok=True)
+    w = cases.ring_stations(stations=40, seed=0)
+    R = O.RefSystem([w], NU)
+    R.integrate("rk4", 0.03, 3, True, str(d / "ring1000_rk4"))
+
+
+if __name__ == "__main__":
+    ring1000()
+    ring5000()
+    twowake()
+    integrate_files()
+    for p in sorted(OUT.rglob("*")):
+        if p.is_file() and p.suffix != ".py":
+            print(p.relative_to(OUT), p.stat().st_size)

@@ -1,0 +1,241 @@
+"""GPU parity: the sm_100a path through the C ABI vs PAWAN's own code.
+
+Gates: FP64 mode within 1e-10 and FP32-compensated mode within 1e-5
+(max-norm relative error, max_i |x_i - ref_i| / max_i |ref_i|), both against
+PAWAN's compiled CPU code or the golden fixtures it produced.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pawan_b200 import capi, cases
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+TOL = {capi.FP64: 1e-10, capi.FP32C: 1e-5}
+PREC = [capi.FP64, capi.FP32C]
+
+
+def golden_wake(name="ring1000.npz"):
+    g = np.load(GOLD / name)
+    return g, cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
+
+
+def ctx_with(wakes, precision, nu, systems=None, capacity=None, **kw):
+    c = capi.Context(precision=precision, nu=nu, **kw)
+    ids = []
+    for i, w in enumerate(wakes):
+        ids.append(c.add_wake(capacity[i] if capacity else w.n, systems[i] if systems else 0))
+    for i, w in zip(ids, wakes):
+        c.set_particles(i, w)
+    return c, ids
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_rates_vs_golden(gpu, prec):
+    g, w = golden_wake()
+    c, _ = ctx_with([w], prec, float(g["nu"]))
+    c.solve()
+    v, a = c.rates(0)
+    assert O.rel_err(v, g["vel"]) < TOL[prec]
+    assert O.rel_err(a, g["dalpha"]) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_rates_ring5000_sampled(gpu, prec):
+    g = np.load(GOLD / "ring5000.npz")
+    w = cases.ring_stations()
+    c, _ = ctx_with([w], prec, float(g["nu"]))
+    c.solve()
+    v, a = c.rates(0)
+    rows = g["rows"]
+    assert O.rel_err(v[rows], g["vel"]) < TOL[prec]
+    assert O.rel_err(a[rows], g["dalpha"]) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PREC)
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_steps_vs_golden(gpu, prec, scheme):
+    g, w = golden_wake()
+    c, _ = ctx_with([w], prec, float(g["nu"]))
+    c.step(scheme, float(g["dt"]), 2)
+    c.sync()
+    x, al = c.state(0)
+    assert O.rel_err(x, g[f"{scheme}_pos"]) < TOL[prec]
+    assert O.rel_err(al, g[f"{scheme}_alpha"]) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_rk4_step_ring5000_sampled(gpu, prec):
+    g = np.load(GOLD / "ring5000.npz")
+    w = cases.ring_stations()
+    c, _ = ctx_with([w], prec, float(g["nu"]))
+    c.step("rk4", float(g["dt"]), 1)
+    x, al = c.state(0)
+    rows = g["rows"]
+    assert O.rel_err(x[rows], g["rk4_pos"]) < TOL[prec]
+    assert O.rel_err(al[rows], g["rk4_alpha"]) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_euler_vs_reference(gpu, ref_available, prec):
+    _, w = golden_wake()
+    R = O.RefSystem([w], 1e-4)
+    R.step("euler", 0.01, 3)
+    xr, ar = R.state()
+    c, _ = ctx_with([w], prec, 1e-4)
+    c.step("euler", 0.01, 3)
+    x, al = c.state(0)
+    assert O.rel_err(x, xr) < TOL[prec]
+    assert O.rel_err(al, ar) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_two_wakes_one_system(gpu, prec):
+    g = np.load(GOLD / "twowake.npz")
+    w1 = cases.Wake(g["pos1"], g["alpha1"], g["sigma1"], g["vol1"])
+    w2 = cases.Wake(g["pos2"], g["alpha2"], g["sigma2"], g["vol2"])
+    c, ids = ctx_with([w1, w2], prec, float(g["nu"]))
+    c.solve()
+    v1, d1 = c.rates(ids[0])
+    v2, d2 = c.rates(ids[1])
+    assert O.rel_err(np.concatenate([v1, v2]), np.concatenate([g["vel1"], g["vel2"]])) < TOL[prec]
+    assert O.rel_err(np.concatenate([d1, d2]), np.concatenate([g["dalpha1"], g["dalpha2"]])) < TOL[prec]
+    d, _ = c.diagnose(0)
+    ref = g["diag"]
+    tol = 1e-9 if prec == capi.FP64 else 1e-4
+    np.testing.assert_allclose(d[3:14], ref[3:14], rtol=tol, atol=tol * np.abs(ref[3:14]).max())
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_diagnostics_vs_golden(gpu, prec):
+    g, w = golden_wake()
+    c, _ = ctx_with([w], prec, float(g["nu"]))
+    d, vbi = c.diagnose(0)
+    ref = g["diag"]
+    # O(N) sums are FP64 in both modes
+    np.testing.assert_allclose(d[3:9], ref[3:9], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(vbi, g["vbi"], rtol=1e-10, atol=1e-14)
+    assert d[10] == 0.0 and d[11] == 0.0
+    tol = 1e-10 if prec == capi.FP64 else 1e-5
+    np.testing.assert_allclose(d[12:14], ref[12:14], rtol=tol)
+    # helicity of a planar ring is a cancelling sum: compare against its scale
+    assert abs(d[9] - ref[9]) < tol * max(abs(ref[9]), 1e-3 * ref[12])
+    assert abs(d[14] - ref[14]) < 1e-9
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_batched_systems_equal_separate(gpu, prec):
+    """Independent systems in one launch give the same rates as one context each."""
+    rings = cases.uneven_rings(count=6, scale=0.02, seed=7)
+    c, ids = ctx_with(rings, prec, 1e-4, systems=list(range(len(rings))))
+    c.solve()
+    for i, w in zip(ids, rings):
+        v, a = c.rates(i)
+        vr, ar = O.restate_rates(w, 1e-4)
+        assert O.rel_err(v, vr) < TOL[prec]
+        assert O.rel_err(a, ar) < TOL[prec]
+
+
+@pytest.mark.parametrize("shape", [(128, 1), (128, 2), (256, 1), (256, 2), (64, 2), (128, 4)])
+def test_every_kernel_shape(gpu, shape):
+    g, w = golden_wake()
+    c, _ = ctx_with([w], capi.FP32C, float(g["nu"]), block=shape[0], tpt=shape[1])
+    c.solve()
+    v, a = c.rates(0)
+    assert O.rel_err(v, g["vel"]) < 1e-5
+    assert O.rel_err(a, g["dalpha"]) < 1e-5
+
+
+def test_graph_and_eager_steps_identical(gpu):
+    _, w = golden_wake()
+    out = []
+    for graphs in (True, False):
+        c, _ = ctx_with([w], capi.FP32C, 1e-4, use_graphs=graphs)
+        c.step("rk4", 0.01, 3)
+        out.append(c.state(0))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 255, 257, 1025])
+def test_ragged_sizes(gpu, n):
+    _, w = golden_wake()
+    ws = w.subset(n)
+    c, _ = ctx_with([ws], capi.FP64, 1e-4, capacity=[n + 100])
+    c.solve()
+    v, a = c.rates(0)
+    vr, ar = O.restate_rates(ws, 1e-4)
+    if n == 1:
+        assert np.all(v == 0) and np.all(a == 0)
+    else:
+        assert O.rel_err(v, vr) < 1e-10 and O.rel_err(a, ar) < 1e-10
+
+
+def test_empty_wake_and_growth(gpu):
+    _, w = golden_wake()
+    c = capi.Context(precision=capi.FP64, nu=1e-4)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w.subset(0))
+    c.solve()
+    c.step("rk4", 0.01, 1)
+    assert c.num_particles(k) == 0
+    c.append_particles(k, w.subset(400))
+    rest = cases.Wake(w.pos[400:], w.alpha[400:], w.sigma[400:], w.vol[400:])
+    c.append_particles(k, rest)
+    c.solve()
+    v, a = c.rates(k)
+    g = np.load(GOLD / "ring1000.npz")
+    assert O.rel_err(v, g["vel"]) < 1e-10 and O.rel_err(a, g["dalpha"]) < 1e-10
+
+
+def test_host_errors(gpu):
+    _, w = golden_wake()
+    c = capi.Context()
+    k = c.add_wake(10)
+    with pytest.raises(capi.PgpuError) as e:
+        c.set_particles(k, w.subset(11))
+    assert e.value.code == capi.PGPU_EINVAL
+    c.set_particles(k, w.subset(10))
+    with pytest.raises(capi.PgpuError):
+        c.add_wake(5)
+    with pytest.raises(capi.PgpuError):
+        c.step("rk4", 0.01, -1)
+    with pytest.raises(capi.PgpuError):
+        c.rates(3)
+
+
+def test_non_finite_state_is_reported(gpu):
+    _, w = golden_wake()
+    bad = w.copy()
+    bad.alpha[5, 0] = np.nan
+    c, _ = ctx_with([bad], capi.FP32C, 1e-4)
+    c.step("euler", 0.01, 1)
+    with pytest.raises(capi.PgpuError) as e:
+        c.sync()
+    assert e.value.code == capi.PGPU_ENUMERIC
+
+
+def test_flat_state_roundtrip(gpu):
+    g, w = golden_wake()
+    c, _ = ctx_with([w], capi.FP64, 1e-4)
+    maxn = [1200]
+    st = c.get_states_flat(maxn)
+    np.testing.assert_array_equal(st[:3000].reshape(-1, 3), w.pos)
+    np.testing.assert_array_equal(st[3600:6600].reshape(-1, 3), w.alpha)
+    c.set_states_flat(st, maxn)
+    c.solve()
+    r = c.get_rates_flat(maxn)
+    assert O.rel_err(r[:3000].reshape(-1, 3), g["vel"]) < 1e-10
+
+
+def test_probe_matches_reference_getvi(gpu, ref_available):
+    _, w = golden_wake()
+    R = O.RefSystem([w], 1e-4)
+    pts = np.array([[0.0, 0.0, 0.0], [0.0, 0.8, 0.0], [-0.255, 0.8, 0.02], [1.0, 0.0, 0.1], [2.0, 1.0, -0.5]])
+    ref = np.array([R.getvi(p) for p in pts])
+    c, _ = ctx_with([w], capi.FP64, 1e-4)
+    v = c.probe(pts)
+    assert O.rel_err(v, ref) < 1e-10
