@@ -143,6 +143,15 @@ int pgpu_autotune(pgpu_ctx *ctx, int reps, int *block, int *tpt, double *ms_per_
 /* Number of compiled pair-kernel shapes and their (block, tpt). */
 int pgpu_kernel_shapes(int *block, int *tpt, int max);
 
+/* The context's CUDA stream (a cudaStream_t), so a caller can order its own
+ * work or timing events with the library's launches.  No PAWAN counterpart. */
+int pgpu_get_stream(pgpu_ctx *ctx, void **stream);
+
+/* Measures the device's sustained FP32 FMA throughput (TFLOP/s, an FMA
+ * counted as 2 flops) with a register-resident FFMA loop on every SM, for
+ * roofline denominators.  No PAWAN counterpart. */
+int pgpu_fp32_peak(int device, double *tflops, double *ms);
+
 const char *pgpu_last_error(pgpu_ctx *ctx);
 const char *pgpu_version(void);
 

@@ -31,7 +31,8 @@ EXPORTS = [
     "pgpu_append_particles", "pgpu_get_num_particles", "pgpu_get_state", "pgpu_set_states_flat",
     "pgpu_get_states_flat", "pgpu_get_rates_flat", "pgpu_solve", "pgpu_get_rates", "pgpu_step",
     "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
-    "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version",
+    "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
+    "pgpu_fp32_peak",
 ]
 
 
@@ -92,6 +93,8 @@ def load(build_if_missing: bool = False):
         "pgpu_kernel_shapes": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
         "pgpu_last_error": (C.c_char_p, [vp]),
         "pgpu_version": (C.c_char_p, []),
+        "pgpu_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
+        "pgpu_fp32_peak": (C.c_int, [C.c_int, _dp, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -107,6 +110,16 @@ def _p(a: np.ndarray):
 
 def _c(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def fp32_peak(device: int = 0) -> float:
+    """Measured FP32 FMA throughput of the device in TFLOP/s."""
+    lib = load()
+    tf, ms = C.c_double(), C.c_double()
+    rc = lib.pgpu_fp32_peak(device, C.byref(tf), C.byref(ms))
+    if rc != PGPU_OK:
+        raise PgpuError(rc, "pgpu_fp32_peak failed")
+    return tf.value
 
 
 def kernel_shapes() -> list[tuple[int, int]]:
@@ -225,6 +238,11 @@ class Context:
         n = C.c_int64()
         self._ck(self.lib.pgpu_pair_kernel_time(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._ck(self.lib.pgpu_get_stream(self.h, C.byref(s)))
+        return int(s.value or 0)
 
     def launch_count(self) -> int:
         return int(self.lib.pgpu_launch_count(self.h))

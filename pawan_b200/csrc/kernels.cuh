@@ -558,4 +558,24 @@ __global__ void __launch_bounds__(BLOCK) probe_kernel(const double *x0, const do
   if (valid) { vel[3 * pi] += u0; vel[3 * pi + 1] += u1; vel[3 * pi + 2] += u2; }
 }
 
+// FP32 pipe throughput probe: kFfmaChains independent FMA chains per thread,
+// all operands in registers.  The result is stored only if it equals a value
+// it cannot take, so the loop is not eliminated.
+constexpr int kFfmaChains = 8;
+__global__ void __launch_bounds__(256) ffma_peak_kernel(float *out, int iters, float a, float b) {
+  float x[kFfmaChains];
+#pragma unroll
+  for (int k = 0; k < kFfmaChains; ++k) x[k] = threadIdx.x * 1e-3f + k;
+  for (int i = 0; i < iters; i += 4) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int k = 0; k < kFfmaChains; ++k) x[k] = fmaf(x[k], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < kFfmaChains; ++k) s += x[k];
+  if (s == -1.2345e30f) *out = s;
+}
+
 }  // namespace pgpu

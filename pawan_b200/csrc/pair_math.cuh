@@ -27,8 +27,9 @@
 // which gives, with u = x^2,
 //   q' = k1 s^3 S(u),   S(u) = sum_k (-1)^k u^k / (2^k k! (2k+3))
 //   F' = -k1 s^5 T(u),  T(u) = sum_m (-1)^m u^m / (2^m m! (2m+5))
-// Both are finite at u = 0, so the self pair (d = 0, a_t x a_s = 0,
-// v_t a_s - v_s a_t = 0) contributes exact zeros without an index mask.
+// Both are finite at u = 0; the series branch (the only one a zero distance
+// reaches) zeroes all three terms at rho = 0, so the self pair contributes
+// exact zeros without an index comparison in the inner loop.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -109,8 +110,12 @@ __device__ __forceinline__ PairTerms<float> pair_terms(float r2, float s2) {
     Tt = fmaf(Tt, u, (float)PGPU_T7); Tt = fmaf(Tt, u, (float)PGPU_T6); Tt = fmaf(Tt, u, (float)PGPU_T5);
     Tt = fmaf(Tt, u, (float)PGPU_T4); Tt = fmaf(Tt, u, (float)PGPU_T3); Tt = fmaf(Tt, u, (float)PGPU_T2);
     Tt = fmaf(Tt, u, (float)PGPU_T1); Tt = fmaf(Tt, u, (float)PGPU_T0);
-    o.q = zk * S;
-    o.F = -zk * is2 * Tt;
+    // rho = 0 only for the self pair (or coincident particles, where PAWAN's
+    // closed form yields NaN): it contributes nothing.
+    const float m = r2 > 0.0f ? 1.0f : 0.0f;
+    o.q = zk * S * m;
+    o.F = -zk * is2 * Tt * m;
+    o.zd = z * is2 * m;
   } else {
     const float ir = fast_rsqrt(r2);
     const float ir2 = ir * ir;
@@ -118,8 +123,8 @@ __device__ __forceinline__ PairTerms<float> pair_terms(float r2, float s2) {
     const float er = erff(y);
     o.q = ir2 * fmaf(-(float)kK1 * is, E, er * ir);
     o.F = fmaf(-3.0f, o.q, z) * ir2;
+    o.zd = z * is2;
   }
-  o.zd = z * is2;
   return o;
 }
 
@@ -138,8 +143,10 @@ __device__ __forceinline__ PairTerms<double> pair_terms(double r2, double s2) {
     double Tt = PGPU_T8;
     Tt = fma(Tt, u, PGPU_T7); Tt = fma(Tt, u, PGPU_T6); Tt = fma(Tt, u, PGPU_T5); Tt = fma(Tt, u, PGPU_T4);
     Tt = fma(Tt, u, PGPU_T3); Tt = fma(Tt, u, PGPU_T2); Tt = fma(Tt, u, PGPU_T1); Tt = fma(Tt, u, PGPU_T0);
-    o.q = zk * S;
-    o.F = -zk * is2 * Tt;
+    const double m = r2 > 0.0 ? 1.0 : 0.0;
+    o.q = zk * S * m;
+    o.F = -zk * is2 * Tt * m;
+    o.zd = z * is2 * m;
   } else {
     const double rho = sqrt(r2);
     const double ir = 1.0 / rho;
@@ -147,8 +154,8 @@ __device__ __forceinline__ PairTerms<double> pair_terms(double r2, double s2) {
     const double er = erf(rho * is * 0.70710678118654752440);
     o.q = ir2 * (er * ir - kK1 * is * E);
     o.F = (z - 3.0 * o.q) * ir2;
+    o.zd = z * is2;
   }
-  o.zd = z * is2;
   return o;
 }
 

@@ -81,6 +81,7 @@ struct pgpu_ctx {
   int nch = 1;
   bool plan_dirty = true;
   bool timing = true;
+  bool capturing = false;
   cudaEvent_t ev[8][2];
   double pair_ms = 0.0;
   int64_t pair_launches = 0;
@@ -264,10 +265,13 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   a.cap = c->cap;
   a.nu2 = (T)(2.0 * c->cfg.nu);
   a.counters = c->d_counters;
-  if (c->timing && slot >= 0) CK(cudaEventRecord(c->ev[slot][0], c->st));
+  // Inside stream capture an event record only becomes a timestamp node of
+  // the graph when it is marked external.
+  const unsigned flags = c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][0], c->st, flags));
   pair_fn<T>(c->shape)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
   CK(cudaGetLastError());
-  if (c->timing && slot >= 0) CK(cudaEventRecord(c->ev[slot][1], c->st));
+  if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][1], c->st, flags));
   c->launches++;
   return PGPU_OK;
 }
@@ -568,7 +572,9 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     const int64_t before = c->launches;
+    c->capturing = true;
     r = record_step(c, scheme, dt);
+    c->capturing = false;
     cudaError_t e = cudaStreamEndCapture(c->st, &g);
     if (r) return r;
     if (e != cudaSuccess) return fail(c, PGPU_ECUDA, "stream capture failed: %s", cudaGetErrorString(e));
@@ -741,6 +747,43 @@ int pgpu_autotune(pgpu_ctx *c, int reps, int *block, int *tpt, double *ms_per_la
   pgpu_pair_kernel_time(c, nullptr, nullptr);
   if (block) *block = kShapes[best_s].block;
   if (tpt) *tpt = kShapes[best_s].tpt;
+  return PGPU_OK;
+}
+
+int pgpu_get_stream(pgpu_ctx *c, void **stream) {
+  if (!c || !stream) return PGPU_EINVAL;
+  *stream = (void *)c->st;
+  return PGPU_OK;
+}
+
+int pgpu_fp32_peak(int device, double *tflops, double *ms_out) {
+  pgpu_ctx *c = nullptr;  // for CK's error path
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float *out = nullptr;
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  CK(cudaMallocAsync((void **)&out, sizeof(float), st));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int block = 256, grid = sms * 8, iters = 1 << 14;
+  ffma_peak_kernel<<<grid, block, 0, st>>>(out, iters, 0.999f, 1e-3f);  // warm-up
+  CK(cudaEventRecord(e0, st));
+  ffma_peak_kernel<<<grid, block, 0, st>>>(out, iters, 0.999f, 1e-3f);
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  const double flops = 2.0 * kFfmaChains * (double)iters * grid * block;
+  if (tflops) *tflops = flops / (ms * 1e-3) / 1e12;
+  if (ms_out) *ms_out = ms;
+  cudaFreeAsync(out, st);
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
   return PGPU_OK;
 }
 

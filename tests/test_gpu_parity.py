@@ -129,7 +129,9 @@ def test_diagnostics_vs_golden(gpu, prec):
 @pytest.mark.parametrize("prec", PREC)
 def test_batched_systems_equal_separate(gpu, prec):
     """Independent systems in one launch give the same rates as one context each."""
-    rings = cases.uneven_rings(count=6, scale=0.02, seed=7)
+    # at least 16 stations per ring: with fewer, strengths are (anti)parallel,
+    # true stretching vanishes and only input rounding is left to compare
+    rings = cases.uneven_rings(count=6, nmin=400, nmax=4000, seed=7)
     c, ids = ctx_with(rings, prec, 1e-4, systems=list(range(len(rings))))
     c.solve()
     for i, w in zip(ids, rings):
