@@ -132,6 +132,13 @@ int pgpu_sync(pgpu_ctx *ctx);
  * (CUDA events on the context stream), and the number of them. */
 int pgpu_pair_kernel_time(pgpu_ctx *ctx, double *ms, int64_t *launches);
 
+/* Ordered pair interactions (self pairs excluded) evaluated by the pair
+ * kernel since the last call, and how many of them took the full formula;
+ * the rest took the far-field limit (FP32C mode, rho^2 >= 50 sigma^2, where
+ * erf rounds to 1 and exp(-rho^2/2sigma^2) < 1.4e-11).  Resets both counts.
+ * No PAWAN counterpart (PAWAN has no counters). */
+int pgpu_pair_counts(pgpu_ctx *ctx, int64_t *pairs, int64_t *full_pairs);
+
 /* Kernel launches issued since context creation (all kernels of this library). */
 int64_t pgpu_launch_count(pgpu_ctx *ctx);
 

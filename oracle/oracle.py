@@ -13,8 +13,10 @@ Only ``tests/``, ``__graft_entry__.smoke`` and the CPU-baseline leg of
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -36,6 +38,25 @@ def _c(a, dtype=np.float64) -> np.ndarray:
 
 _ref = None
 _rs = None
+
+
+@contextlib.contextmanager
+def quiet():
+    """Sends the process's stdout (file descriptor 1) to /dev/null: PAWAN's
+    classes print progress with printf / std::cout."""
+    libc = C.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
 
 
 def ref_available() -> bool:

@@ -32,7 +32,7 @@ EXPORTS = [
     "pgpu_get_states_flat", "pgpu_get_rates_flat", "pgpu_solve", "pgpu_get_rates", "pgpu_step",
     "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
     "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
-    "pgpu_fp32_peak",
+    "pgpu_fp32_peak", "pgpu_pair_counts",
 ]
 
 
@@ -95,6 +95,7 @@ def load(build_if_missing: bool = False):
         "pgpu_version": (C.c_char_p, []),
         "pgpu_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
         "pgpu_fp32_peak": (C.c_int, [C.c_int, _dp, _dp]),
+        "pgpu_pair_counts": (C.c_int, [vp, _i64p, _i64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -243,6 +244,12 @@ class Context:
         s = C.c_void_p()
         self._ck(self.lib.pgpu_get_stream(self.h, C.byref(s)))
         return int(s.value or 0)
+
+    def pair_counts(self) -> tuple[int, int]:
+        """(ordered pairs, full-formula pairs) evaluated since the last call."""
+        p, f = C.c_int64(), C.c_int64()
+        self._ck(self.lib.pgpu_pair_counts(self.h, C.byref(p), C.byref(f)))
+        return p.value, f.value
 
     def launch_count(self) -> int:
         return int(self.lib.pgpu_launch_count(self.h))

@@ -51,6 +51,7 @@ template <typename T> struct PairArgs {
   int64_t cap;
   T nu2;  // 2 nu
   unsigned int *counters;  // [0] next item, [1] finished CTAs
+  unsigned long long *nfull;  // accumulated count of full-formula pairs
 };
 
 // ---------------------------------------------------------------- helpers
@@ -146,6 +147,7 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
 
     T xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT];
     T vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
+    unsigned nfull = 0;  // pairs evaluated with the full (non-far) formula, self pairs included
 #pragma unroll
     for (int k = 0; k < TPT; ++k) {
       int64_t ti = t0 + tid + k * BLOCK;
@@ -180,12 +182,11 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
 
 #pragma unroll 1
       for (int g = 0; g < TILE; g += CG) {
-        T sv[TPT][3], sd[TPT][3], sp[TPT][3], sdv[TPT][3], sds[TPT];
+        T sv[TPT][3], sd[TPT][3], sp[TPT][3], sdv[TPT][3];
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
 #pragma unroll
           for (int m = 0; m < 3; ++m) { sv[k][m] = 0; sd[k][m] = 0; sp[k][m] = 0; sdv[k][m] = 0; }
-          sds[k] = 0;
         }
 #pragma unroll 4
         for (int jj = 0; jj < CG; ++jj) {
@@ -195,26 +196,53 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
           for (int k = 0; k < TPT; ++k) {
             const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
             const T r2 = dx * dx + dy * dy + dz * dz;
-            const PairTerms<T> pt = pair_terms(r2, hst[k] + p.w);
+            const T s2 = hst[k] + p.w;
+            T qq, FF;
+            bool diffuse;
+            T zd = 0;
+            if constexpr (sizeof(T) == 4) {
+              if (r2 >= kFarU * s2) {
+                // far limit: q' = r^3, F' = -3 r^5, no diffusion
+                const float ir = fast_rsqrt(r2);
+                const float A = ir * ir;
+                qq = A * ir;
+                FF = -3.0f * qq * A;
+                diffuse = false;
+              } else {
+                const PairTerms<float> pt = pair_terms_near(r2, s2);
+                qq = pt.q; FF = pt.F; zd = pt.zd;
+                diffuse = true;
+                ++nfull;
+              }
+            } else {
+              const PairTerms<T> pt = pair_terms(r2, s2);
+              qq = pt.q; FF = pt.F; zd = pt.zd;
+              diffuse = true;
+            }
             // w = alpha_s x d
             const T wx = q.y * dz - q.z * dy;
             const T wy = q.z * dx - q.x * dz;
             const T wz = q.x * dy - q.y * dx;
-            sv[k][0] += pt.q * wx; sv[k][1] += pt.q * wy; sv[k][2] += pt.q * wz;
+            sv[k][0] += qq * wx; sv[k][1] += qq * wy; sv[k][2] += qq * wz;
             // d . (alpha_t x alpha_s) = alpha_t . w
-            const T fd = pt.F * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
+            const T fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
             sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
-            sp[k][0] += pt.q * q.x; sp[k][1] += pt.q * q.y; sp[k][2] += pt.q * q.z;
-            sdv[k][0] += pt.zd * q.x; sdv[k][1] += pt.zd * q.y; sdv[k][2] += pt.zd * q.z;
-            sds[k] += pt.zd * q.w;
+            sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
+            if (diffuse) {
+              // v_t a_s - v_s a_t per pair, so nearly equal strengths cancel
+              // before they are summed (as in DIFFUSION, interaction_utils.h:358-369)
+              sdv[k][0] += zd * (vt[k] * q.x - q.w * at[k][0]);
+              sdv[k][1] += zd * (vt[k] * q.y - q.w * at[k][1]);
+              sdv[k][2] += zd * (vt[k] * q.z - q.w * at[k][2]);
+            }
           }
         }
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
-          // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu (v_t sum z alpha_s - alpha_t sum z v_s)
-          const T ex = at[k][1] * sp[k][2] - at[k][2] * sp[k][1] + sd[k][0] + a.nu2 * (vt[k] * sdv[k][0] - sds[k] * at[k][0]);
-          const T ey = at[k][2] * sp[k][0] - at[k][0] * sp[k][2] + sd[k][1] + a.nu2 * (vt[k] * sdv[k][1] - sds[k] * at[k][1]);
-          const T ez = at[k][0] * sp[k][1] - at[k][1] * sp[k][0] + sd[k][2] + a.nu2 * (vt[k] * sdv[k][2] - sds[k] * at[k][2]);
+          // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t)
+          const T ex = at[k][1] * sp[k][2] - at[k][2] * sp[k][1] + sd[k][0] + a.nu2 * sdv[k][0];
+          const T ey = at[k][2] * sp[k][0] - at[k][0] * sp[k][2] + sd[k][1] + a.nu2 * sdv[k][1];
+          const T ez = at[k][0] * sp[k][1] - at[k][1] * sp[k][0] + sd[k][2] + a.nu2 * sdv[k][2];
           two_sum_acc(vh[k][0], vl[k][0], sv[k][0]);
           two_sum_acc(vh[k][1], vl[k][1], sv[k][1]);
           two_sum_acc(vh[k][2], vl[k][2], sv[k][2]);
@@ -227,6 +255,11 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
       buf ^= 1;
     }
     cp_async_wait<0>();
+    if constexpr (sizeof(T) == 4) {
+      const unsigned wsum = __reduce_add_sync(0xffffffffu, nfull);
+      if ((tid & 31) == 0 && wsum) atomicAdd(a.nfull, (unsigned long long)wsum);
+      nfull = 0;
+    }
 
 #pragma unroll
     for (int k = 0; k < TPT; ++k) {

@@ -74,6 +74,8 @@ struct pgpu_ctx {
   int64_t *d_sysoff = nullptr, *d_sysn = nullptr;
   PlanEntry *d_plan = nullptr, *d_plan_diag = nullptr;
   unsigned int *d_counters = nullptr;
+  unsigned long long *d_nfull = nullptr;
+  int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
   int *d_flag = nullptr;
   int diag_blocks = 0;
   int shape = 3;
@@ -176,6 +178,7 @@ int freeze(pgpu_ctx *c) {
   if ((r = alloc((void **)&c->d_plan, (ns + 1) * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_plan_diag, 2 * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_counters, 4 * sizeof(unsigned int)))) return r;
+  if ((r = alloc((void **)&c->d_nfull, sizeof(unsigned long long)))) return r;
   if ((r = alloc((void **)&c->d_flag, sizeof(int)))) return r;
   c->diag_blocks = 2 * c->sms;
   if ((r = alloc((void **)&c->d_diag, (size_t)c->diag_blocks * kDiagFields * sizeof(double)))) return r;
@@ -186,6 +189,7 @@ int freeze(pgpu_ctx *c) {
   CK(cudaMemsetAsync(c->vol, 0, cap * sizeof(double), c->st));
   CK(cudaMemsetAsync(c->partial, 0, (size_t)kMaxChunks * 6 * cap * sizeof(double), c->st));
   CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned int), c->st));
+  CK(cudaMemsetAsync(c->d_nfull, 0, sizeof(unsigned long long), c->st));
   CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->st));
   for (int s = 0; s < kNumShapes; ++s) c->grid[s] = fp64(c) ? occupancy<double>(c, s) : occupancy<float>(c, s);
   c->frozen = true;
@@ -254,6 +258,14 @@ int upload_plan(pgpu_ctx *c) {
   return PGPU_OK;
 }
 
+void account_pairs(pgpu_ctx *c, int launches) {
+  for (size_t s = 0; s < c->sys.size(); ++s) {
+    const int64_t n = sys_n(c, (int)s);
+    c->pairs_acc += launches * n * (n > 0 ? n - 1 : 0);
+    c->selfs_acc += launches * n;
+  }
+}
+
 template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   PairArgs<T> a;
   a.P = static_cast<const v4_t<T> *>(c->P);
@@ -265,6 +277,7 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   a.cap = c->cap;
   a.nu2 = (T)(2.0 * c->cfg.nu);
   a.counters = c->d_counters;
+  a.nfull = c->d_nfull;
   // Inside stream capture an event record only becomes a timestamp node of
   // the graph when it is marked external.
   const unsigned flags = c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
@@ -273,6 +286,7 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   CK(cudaGetLastError());
   if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][1], c->st, flags));
   c->launches++;
+  if (!c->capturing) account_pairs(c, 1);
   return PGPU_OK;
 }
 
@@ -412,7 +426,7 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
-                  c->d_sysoff, c->d_sysn, c->d_plan, c->d_plan_diag, c->d_counters, c->d_flag};
+                  c->d_sysoff, c->d_sysn, c->d_plan, c->d_plan_diag, c->d_counters, c->d_nfull, c->d_flag};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
@@ -587,6 +601,7 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
   for (int i = 0; i < nsteps; ++i) {
     CK(cudaGraphLaunch(it->second, c->st));
     c->launches += 2 * ns;
+    account_pairs(c, ns);
     if ((r = collect_timing(c, ns))) return r;
   }
   return PGPU_OK;
@@ -702,6 +717,23 @@ int pgpu_pair_kernel_time(pgpu_ctx *c, double *ms, int64_t *launches) {
 }
 
 int64_t pgpu_launch_count(pgpu_ctx *c) { return c ? c->launches : -1; }
+
+int pgpu_pair_counts(pgpu_ctx *c, int64_t *pairs, int64_t *full_pairs) {
+  if (!c) return PGPU_EINVAL;
+  int64_t full = c->pairs_acc;
+  if (c->frozen && !fp64(c)) {
+    unsigned long long nf = 0;
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaMemcpy(&nf, c->d_nfull, sizeof(nf), cudaMemcpyDeviceToHost));
+    CK(cudaMemset(c->d_nfull, 0, sizeof(nf)));
+    full = (int64_t)nf - c->selfs_acc;
+  }
+  if (pairs) *pairs = c->pairs_acc;
+  if (full_pairs) *full_pairs = full;
+  c->pairs_acc = 0;
+  c->selfs_acc = 0;
+  return PGPU_OK;
+}
 
 int pgpu_kernel_shapes(int *block, int *tpt, int max) {
   for (int s = 0; s < kNumShapes && s < max; ++s) {
