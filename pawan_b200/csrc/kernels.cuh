@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
     const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
     const int64_t s1 = min(s0 + pe.chunk, tend);
 
-    T xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT];
+    T xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT], h50[TPT];
     T vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
     unsigned nfull = 0;  // pairs evaluated with the full (non-far) formula, self pairs included
 #pragma unroll
@@ -155,6 +155,7 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
       const v4_t<T> p = a.P[ti];
       const v4_t<T> q = a.Q[ti];
       xt[k][0] = p.x; xt[k][1] = p.y; xt[k][2] = p.z; hst[k] = p.w;
+      h50[k] = T(kFarU) * p.w;
       at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
 #pragma unroll
       for (int m = 0; m < 3; ++m) { vh[k][m] = 0; vl[k][m] = 0; dh[k][m] = 0; dl[k][m] = 0; }
@@ -196,26 +197,31 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
           for (int k = 0; k < TPT; ++k) {
             const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
             const T r2 = dx * dx + dy * dy + dz * dz;
-            const T s2 = hst[k] + p.w;
             T qq, FF;
             bool diffuse;
             T zd = 0;
             if constexpr (sizeof(T) == 4) {
-              if (r2 >= kFarU * s2) {
-                // far limit: q' = r^3, F' = -3 r^5, no diffusion
-                const float ir = fast_rsqrt(r2);
-                const float A = ir * ir;
-                qq = A * ir;
-                FF = -3.0f * qq * A;
-                diffuse = false;
-              } else {
-                const PairTerms<float> pt = pair_terms_near(r2, s2);
-                qq = pt.q; FF = pt.F; zd = pt.zd;
-                diffuse = true;
-                ++nfull;
+              // far test r^2 >= 50 (hs_t + hs_s) as one FMA against the
+              // target's precomputed 50 hs_t
+              const bool near = fmaf(-kFarU, p.w, r2) < h50[k];
+              // far limit for every lane: q' = r^3, F' = -3 r^5, no diffusion
+              const float ir = fast_rsqrt(r2);
+              const float A = ir * ir;
+              qq = A * ir;
+              FF = -3.0f * qq * A;
+              diffuse = false;
+              // the full formula only when some lane of the warp needs it:
+              // the vote keeps the common all-far case free of divergence
+              if (__any_sync(0xffffffffu, near)) {
+                if (near) {
+                  const PairTerms<float> pt = pair_terms_near(r2, hst[k] + p.w);
+                  qq = pt.q; FF = pt.F; zd = pt.zd;
+                  diffuse = true;
+                  ++nfull;
+                }
               }
             } else {
-              const PairTerms<T> pt = pair_terms(r2, s2);
+              const PairTerms<T> pt = pair_terms(r2, hst[k] + p.w);
               qq = pt.q; FF = pt.F; zd = pt.zd;
               diffuse = true;
             }

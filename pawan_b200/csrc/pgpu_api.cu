@@ -78,7 +78,7 @@ struct pgpu_ctx {
   int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
   int *d_flag = nullptr;
   int diag_blocks = 0;
-  int shape = 3;
+  int shape = 2;  // (256, 1): the fastest shape at 1M particles before autotuning
   int grid[kNumShapes] = {0};
   int nch = 1;
   bool plan_dirty = true;
