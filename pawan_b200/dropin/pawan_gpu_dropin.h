@@ -1,0 +1,86 @@
+/*
+ * Drop-in GPU backend for PAWAN's C++ class surface.
+ *
+ * Compiled inside a PAWAN build (against PAWAN's own headers and GSL) and
+ * linked with libpawan_gpu.so.  Selecting the GPU is then a one-line change
+ * in a PAWAN driver (src/pawan.cpp:47-48):
+ *
+ *     pawan::__interaction *S = new pawan::__parallel(W);     // CPU, OpenMP
+ *     pawan::__interaction *S = new pawan::__gpu(W, cfg);      // B200
+ *     pawan::__integration *IN = new pawan::__rk4(T, n);       // CPU stages
+ *     pawan::__integration *IN = new pawan::__rk4gpu(T, n);    // stages on the GPU
+ *     IN->integrate(S, IO, true);                              // unchanged
+ *
+ * __gpu overrides the virtual members of __interaction that carry the hot
+ * path (interaction.h:192-241): solve, diagnose, addWake.  Particle data stays
+ * authoritative in the host __wake matrices, exactly as in PAWAN; every solve
+ * uploads the current positions/strengths and writes the rates back into
+ * __wake::_velocity / _retvorcity, so getRates/getStates/setStates/write keep
+ * PAWAN's own behaviour.  __rk4gpu / __rk3gpu override the protected step()
+ * (integration.h:37, rk4.h:25, rk3.h:25): the whole step runs on the device
+ * (one CUDA graph per step), and the state vector and the wakes are updated
+ * afterwards, as PAWAN's step leaves them (rk4.cpp:66-68).
+ *
+ * Errors: a non-zero pgpu_* status becomes std::runtime_error carrying
+ * pgpu_last_error().  A GPU integrator given a system that is not a __gpu
+ * throws std::invalid_argument (there is no CPU fallback).
+ */
+#ifndef PAWAN_GPU_DROPIN_H_
+#define PAWAN_GPU_DROPIN_H_
+
+#include <vector>
+
+#include "pawan_gpu.h"
+#include "src/integration/rk3.h"
+#include "src/integration/rk4.h"
+#include "src/interaction/interaction.h"
+
+namespace pawan {
+
+class __gpu : public __interaction {
+ public:
+  __gpu(__wake *W, const pgpu_config &cfg);
+  __gpu(__wake *W1, __wake *W2, const pgpu_config &cfg);
+  ~__gpu();
+
+  void addWake(__wake *W) override;
+  void solve() override;
+  void diagnose() override;
+
+  // Advances the wakes `nsteps` steps on the device (scheme PGPU_RK3 / PGPU_RK4
+  // / PGPU_EULER) starting from the host wakes, then writes the new state back
+  // into them.
+  void device_step(int scheme, double dt, int nsteps);
+  // Velocity induced at npts points (row-major) by all wakes, each particle
+  // with its own radius (getVi, interaction.cpp:453-477).
+  void probe(const double *pts, long npts, double *vel);
+  pgpu_ctx *context() { return _ctx; }
+
+ private:
+  void check(int rc) const;
+  void layout();  // creates the device wakes on first use
+  void upload();
+  void download_state();
+  pgpu_config _cfg;
+  pgpu_ctx *_ctx = nullptr;
+  std::vector<__wake *> _wakes;
+  std::vector<int32_t> _ids;
+  bool _laid_out = false;
+};
+
+class __rk4gpu : public __rk4 {
+ public:
+  __rk4gpu(const double &t, const size_t &n) : __rk4(t, n) {}
+ protected:
+  void step(const double &dt, __system *S, gsl_vector *state) override;
+};
+
+class __rk3gpu : public __rk3 {
+ public:
+  __rk3gpu(const double &t, const size_t &n) : __rk3(t, n) {}
+ protected:
+  void step(const double &dt, __system *S, gsl_vector *state) override;
+};
+
+}  // namespace pawan
+#endif

@@ -1,0 +1,102 @@
+"""The C++ drop-in (pawan::__gpu, __rk4gpu, __rk3gpu) inside PAWAN's own time
+loop __integration::integrate, against PAWAN's own __parallel + __rk4/__rk3.
+
+The driver (tests/dropin/dropin_check.cpp) is compiled against PAWAN's headers
+by tests/dropin/Makefile; it needs the PAWAN sources, so it is built where they
+are and the binary is reused elsewhere.
+"""
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pawan_b200 import cases, wakeio
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLD = ROOT / "tests" / "golden"
+DRIVER = ROOT / "tests" / "_build" / "dropin_check"
+
+
+@pytest.fixture(scope="module")
+def driver():
+    if not DRIVER.exists():
+        if not Path("/root/reference").exists():
+            pytest.skip("drop-in driver not built and PAWAN sources absent")
+        env = {k: v for k, v in os.environ.items() if k not in ("CXX", "CC")}
+        subprocess.run(["make", "-C", str(ROOT / "tests" / "dropin")], check=True, env=env, capture_output=True)
+    return DRIVER
+
+
+def run(driver, tmp_path, mode, scheme, w, dt, nsteps, nu=1e-4):
+    pb = tmp_path / "particles.bin"
+    wakeio.write_particles_bin(pb, w)
+    out = tmp_path / f"{mode}_{scheme}"
+    r = subprocess.run([str(driver), mode, scheme, str(pb), repr(dt), str(nsteps), str(out), repr(nu)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return wakeio.read_wake(str(out) + ".wake"), wakeio.read_diagnosis(str(out) + ".diagnosis")
+
+
+def test_reader_on_reference_files():
+    recs = wakeio.read_wake(GOLD / "integrate" / "ring1000_rk4.wake")
+    assert len(recs) == 4
+    assert [round(t, 12) for t, _ in recs] == [0.0, 0.01, 0.02, 0.03]
+    assert all(len(ws) == 1 and ws[0].n == 1000 for _, ws in recs)
+    nu, d = wakeio.read_diagnosis(GOLD / "integrate" / "ring1000_rk4.diagnosis")
+    assert nu == 1e-4 and d.shape == (4, 16)
+    g = np.load(GOLD / "ring1000.npz")
+    np.testing.assert_allclose(d[0, 4:], g["diag"][3:], rtol=1e-10, atol=1e-14)
+    assert O.rel_err(recs[2][1][0].pos, g["rk4_pos"]) < 1e-13
+
+
+def test_writer_roundtrip(tmp_path):
+    recs = wakeio.read_wake(GOLD / "integrate" / "ring1000_rk4.wake")
+    p = tmp_path / "x.wake"
+    with open(p, "wb") as f:
+        for t, ws in recs:
+            wakeio.write_wake_record(f, t, ws, ws[0].pos.shape[0])
+    back = wakeio.read_wake(p)
+    for (t0, a), (t1, b) in zip(recs, back):
+        assert t0 == t1
+        np.testing.assert_array_equal(a[0].pos, b[0].pos)
+        np.testing.assert_array_equal(a[0].volume, b[0].volume)
+    # byte-identical except the undefined high half of each maxN field
+    raw0 = bytearray((GOLD / "integrate" / "ring1000_rk4.wake").read_bytes())
+    raw1 = bytearray(p.read_bytes())
+    rec = len(raw0) // 4
+    for k in range(4):
+        raw0[k * rec + 20: k * rec + 24] = b"\0\0\0\0"
+    assert raw0 == raw1
+
+
+def test_driver_reference_mode_reproduces_golden(driver, tmp_path, ref_available):
+    g = np.load(GOLD / "ring1000.npz")
+    w = cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
+    recs, (nu, d) = run(driver, tmp_path, "ref", "rk4", w, 0.01, 3)
+    gold = wakeio.read_wake(GOLD / "integrate" / "ring1000_rk4.wake")
+    _, gd = wakeio.read_diagnosis(GOLD / "integrate" / "ring1000_rk4.diagnosis")
+    for (_, a), (_, b) in zip(recs, gold):
+        assert O.rel_err(a[0].pos, b[0].pos) < 1e-13
+        assert O.rel_err(a[0].alpha, b[0].alpha) < 1e-12
+    np.testing.assert_allclose(d[:, 4:], gd[:, 4:], rtol=1e-10, atol=1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,tol", [("gpu64", 1e-10), ("gpu", 1e-5)])
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_dropin_matches_reference_in_pawan_time_loop(gpu, driver, tmp_path, ref_available, mode, tol, scheme):
+    g = np.load(GOLD / "ring1000.npz")
+    w = cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
+    ref, (_, dref) = run(driver, tmp_path, "ref", scheme, w, 0.01, 3)
+    got, (nu, dgot) = run(driver, tmp_path, mode, scheme, w, 0.01, 3)
+    assert nu == 1e-4 and len(got) == len(ref) == 4
+    for (t0, a), (t1, b) in zip(got, ref):
+        assert t0 == t1
+        assert O.rel_err(a[0].pos, b[0].pos) < tol
+        assert O.rel_err(a[0].alpha, b[0].alpha) < tol
+    # diagnostics: O(N) impulses in FP64 on both sides; KE/KEF to the mode's tolerance
+    np.testing.assert_allclose(dgot[:, 4:10], dref[:, 4:10], rtol=max(tol, 1e-10), atol=1e-12)
+    np.testing.assert_allclose(dgot[:, 13:15], dref[:, 13:15], rtol=max(tol, 1e-10))

@@ -241,3 +241,44 @@ def test_probe_matches_reference_getvi(gpu, ref_available):
     c, _ = ctx_with([w], capi.FP64, 1e-4)
     v = c.probe(pts)
     assert O.rel_err(v, ref) < 1e-10
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_inflow_operator_split(gpu, prec):
+    """x += vinf dt after every step (updateVinfEffect, wake.cpp:564-577): a uniform
+    shift leaves the interaction unchanged, so the state is the no-inflow state
+    moved by vinf * t."""
+    _, w = golden_wake()
+    vinf = (0.01, -0.02, -0.05)
+    out = []
+    for v in ((0.0, 0.0, 0.0), vinf):
+        c, _ = ctx_with([w], prec, 1e-4, vinf=v)
+        c.step("rk3", 0.01, 4)
+        out.append(c.state(0))
+    np.testing.assert_allclose(out[1][0] - out[0][0], np.tile(np.array(vinf) * 0.04, (w.n, 1)), atol=1e-12)
+    assert O.rel_err(out[1][1], out[0][1]) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_growing_wake_matches_restatement(gpu, prec):
+    """A wake that gains particles between RK3 steps (the growing rotor wake)
+    replays the same captured step graph and matches the FP64 restatement
+    stepping the same sequence."""
+    sh = cases.RotorShedder(per_blade=40)
+    c = capi.Context(precision=prec, nu=1e-4)
+    k = c.add_wake(4 * 40 * 6)
+    c.set_particles(k, sh.shed())
+    first = cases.RotorShedder(per_blade=40)
+    w_ref = first.shed()
+    for it in range(5):
+        c.step("rk3", sh.dt, 1)
+        x, al = O.restate_step(w_ref, 1e-4, "rk3", sh.dt, 1)
+        w_ref = cases.Wake(x, al, w_ref.sigma, w_ref.vol)
+        new = sh.shed()
+        first.shed()
+        c.append_particles(k, new)
+        w_ref = cases.Wake.concat([w_ref, new])
+    x, al = c.state(k)
+    assert x.shape[0] == w_ref.n == 4 * 40 * 6
+    assert O.rel_err(x, w_ref.pos) < TOL[prec]
+    assert O.rel_err(al, w_ref.alpha) < TOL[prec]
