@@ -255,7 +255,9 @@ def test_inflow_operator_split(gpu, prec):
         c, _ = ctx_with([w], prec, 1e-4, vinf=v)
         c.step("rk3", 0.01, 4)
         out.append(c.state(0))
-    np.testing.assert_allclose(out[1][0] - out[0][0], np.tile(np.array(vinf) * 0.04, (w.n, 1)), atol=1e-12)
+    # FP32C rounds the shifted positions differently, so only FP64 is exact to rounding
+    atol = 1e-12 if prec == capi.FP64 else 1e-6
+    np.testing.assert_allclose(out[1][0] - out[0][0], np.tile(np.array(vinf) * 0.04, (w.n, 1)), atol=atol)
     assert O.rel_err(out[1][1], out[0][1]) < TOL[prec]
 
 
