@@ -150,6 +150,45 @@ int pgpu_autotune(pgpu_ctx *ctx, int reps, int *block, int *tpt, double *ms_per_
 /* Number of compiled pair-kernel shapes and their (block, tpt). */
 int pgpu_kernel_shapes(int *block, int *tpt, int max);
 
+/* ---------------------------------------------------------------------------
+ * Far-field surrogate (no PAWAN counterpart: PAWAN only has the O(N^2) sum).
+ *
+ * With the surrogate enabled, every rate evaluation of the context's single
+ * system uses an octree: each target leaf's near field (cells closer than
+ * near_widths cube widths) is summed exactly with the direct kernel's terms,
+ * and farther cells act through their multipole moments (order 0/1/2),
+ * optionally corrected by the learned model of pgpu_surrogate_set_mlp.  After
+ * every evaluation, check_targets sampled targets are recomputed by the direct
+ * sum; if the max-norm relative velocity error exceeds `tolerance`, the
+ * evaluation is redone by the direct sum (the surrogate never returns an
+ * unchecked result when check_targets > 0). */
+typedef struct pgpu_surrogate_config {
+  int leaf_size;       /* particles per octree leaf, 1..512 (default 512) */
+  double near_widths;  /* near field: cells closer than this many cube widths (default 4) */
+  int order;           /* far-field expansion: 0 monopole, 1 + dipole (default), 2 + quadrupole */
+  int use_mlp;         /* add the learned correction (needs pgpu_surrogate_set_mlp) */
+  double tolerance;    /* maximum relative velocity error on the sampled targets (default 1e-4) */
+  int check_targets;   /* targets re-checked by the direct sum per evaluation (default 4096, 0 = off) */
+  int seed;            /* seed of the sampled targets */
+} pgpu_surrogate_config;
+
+typedef struct pgpu_surrogate_stats {
+  int64_t evaluations;     /* surrogate evaluations since enable */
+  int64_t fallbacks;       /* evaluations redone by the direct sum */
+  double last_err_vel;     /* sampled max-norm relative velocity error of the last evaluation */
+  double last_err_dalpha;  /* same for dalpha/dt */
+  double max_err_vel;      /* largest sampled velocity error seen */
+  double ms_tree, ms_eval, ms_check, ms_fallback;  /* device time of the last evaluation's phases */
+  int64_t cells, leaves;   /* octree of the last evaluation */
+  int64_t far_entries, near_entries;  /* interaction-list lengths summed over leaves */
+} pgpu_surrogate_stats;
+
+void pgpu_surrogate_config_default(pgpu_surrogate_config *cfg);
+/* Enables the surrogate for `system`, which must be the context's only system. */
+int pgpu_surrogate_enable(pgpu_ctx *ctx, int32_t system, const pgpu_surrogate_config *cfg);
+int pgpu_surrogate_disable(pgpu_ctx *ctx);
+int pgpu_surrogate_get_stats(pgpu_ctx *ctx, pgpu_surrogate_stats *stats);
+
 /* The context's CUDA stream (a cudaStream_t), so a caller can order its own
  * work or timing events with the library's launches.  No PAWAN counterpart. */
 int pgpu_get_stream(pgpu_ctx *ctx, void **stream);

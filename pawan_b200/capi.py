@@ -32,13 +32,30 @@ EXPORTS = [
     "pgpu_get_states_flat", "pgpu_get_rates_flat", "pgpu_solve", "pgpu_get_rates", "pgpu_step",
     "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
     "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
-    "pgpu_fp32_peak", "pgpu_pair_counts",
+    "pgpu_fp32_peak", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
+    "pgpu_surrogate_disable", "pgpu_surrogate_get_stats",
 ]
 
 
 class PgpuConfig(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("nu", C.c_double), ("vinf", C.c_double * 3),
                 ("block", C.c_int), ("tpt", C.c_int), ("chunks", C.c_int), ("use_graphs", C.c_int)]
+
+
+class SurrogateConfig(C.Structure):
+    _fields_ = [("leaf_size", C.c_int), ("near_widths", C.c_double), ("order", C.c_int), ("use_mlp", C.c_int),
+                ("tolerance", C.c_double), ("check_targets", C.c_int), ("seed", C.c_int)]
+
+
+class SurrogateStats(C.Structure):
+    _fields_ = [("evaluations", C.c_int64), ("fallbacks", C.c_int64), ("last_err_vel", C.c_double),
+                ("last_err_dalpha", C.c_double), ("max_err_vel", C.c_double), ("ms_tree", C.c_double),
+                ("ms_eval", C.c_double), ("ms_check", C.c_double), ("ms_fallback", C.c_double),
+                ("cells", C.c_int64), ("leaves", C.c_int64), ("far_entries", C.c_int64),
+                ("near_entries", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class PgpuError(RuntimeError):
@@ -96,6 +113,10 @@ def load(build_if_missing: bool = False):
         "pgpu_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
         "pgpu_fp32_peak": (C.c_int, [C.c_int, _dp, _dp]),
         "pgpu_pair_counts": (C.c_int, [vp, _i64p, _i64p]),
+        "pgpu_surrogate_config_default": (None, [C.POINTER(SurrogateConfig)]),
+        "pgpu_surrogate_enable": (C.c_int, [vp, C.c_int32, C.POINTER(SurrogateConfig)]),
+        "pgpu_surrogate_disable": (C.c_int, [vp]),
+        "pgpu_surrogate_get_stats": (C.c_int, [vp, C.POINTER(SurrogateStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -250,6 +271,22 @@ class Context:
         p, f = C.c_int64(), C.c_int64()
         self._ck(self.lib.pgpu_pair_counts(self.h, C.byref(p), C.byref(f)))
         return p.value, f.value
+
+    # ------------------------------------------------------------ far-field surrogate
+    def surrogate_enable(self, system: int = 0, **kw):
+        cfg = SurrogateConfig()
+        self.lib.pgpu_surrogate_config_default(C.byref(cfg))
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        self._ck(self.lib.pgpu_surrogate_enable(self.h, system, C.byref(cfg)))
+
+    def surrogate_disable(self):
+        self._ck(self.lib.pgpu_surrogate_disable(self.h))
+
+    def surrogate_stats(self) -> dict:
+        st = SurrogateStats()
+        self._ck(self.lib.pgpu_surrogate_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
 
     def launch_count(self) -> int:
         return int(self.lib.pgpu_launch_count(self.h))

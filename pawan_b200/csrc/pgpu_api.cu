@@ -23,6 +23,9 @@
 
 #include "../../include/pawan_gpu.h"
 #include "kernels.cuh"
+#include "treeeval.cuh"
+
+#include <cub/cub.cuh>
 
 using namespace pgpu;
 
@@ -60,6 +63,8 @@ struct SysRec {
 
 }  // namespace
 
+struct SurrogateState;
+
 struct pgpu_ctx {
   pgpu_config cfg;
   cudaStream_t st = nullptr;
@@ -91,6 +96,7 @@ struct pgpu_ctx {
   std::map<std::tuple<int, double, int, int>, cudaGraphExec_t> graphs;
   std::vector<cudaGraph_t> graph_defs;
   std::string err;
+  SurrogateState *sur = nullptr;  // far-field surrogate of the single system, when enabled
 };
 
 namespace {
@@ -240,7 +246,8 @@ int upload_plan(pgpu_ctx *c) {
   if (!c->plan_dirty) return PGPU_OK;
   int r = check_contiguous(c);
   if (r) return r;
-  c->nch = choose_nch(c, c->shape);
+  // the surrogate writes one chunk of rates per evaluation
+  c->nch = c->sur ? 1 : choose_nch(c, c->shape);
   std::vector<int> all(c->sys.size());
   for (size_t s = 0; s < all.size(); ++s) all[s] = (int)s;
   std::vector<PlanEntry> plan = build_plan(c, all, c->shape, c->nch);
@@ -318,12 +325,16 @@ int launch_pack(pgpu_ctx *c, int64_t lo, int64_t hi) {
   return PGPU_OK;
 }
 
+int surrogate_eval(pgpu_ctx *c);
+void surrogate_free(pgpu_ctx *c);
+
 int launch_eval(pgpu_ctx *c, int slot) {
+  if (c->sur) return surrogate_eval(c);
   return fp64(c) ? launch_pair<double>(c, slot) : launch_pair<float>(c, slot);
 }
 
 int collect_timing(pgpu_ctx *c, int nslots) {
-  if (!c->timing) return PGPU_OK;
+  if (!c->timing || c->sur) return PGPU_OK;  // surrogate evaluations keep their own phase times
   for (int k = 0; k < nslots; ++k) {
     CK(cudaEventSynchronize(c->ev[k][1]));
     float ms = 0.f;
@@ -423,6 +434,7 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
 int pgpu_destroy(pgpu_ctx *c) {
   if (!c) return PGPU_EINVAL;
   cudaStreamSynchronize(c->st);
+  surrogate_free(c);
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
@@ -573,7 +585,7 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
   int r = upload_plan(c);
   if (r) return r;
   const int ns = stages_of(scheme);
-  if (!c->cfg.use_graphs) {
+  if (!c->cfg.use_graphs || c->sur) {  // the surrogate's tree build synchronises with the host
     for (int i = 0; i < nsteps; ++i) {
       if ((r = record_step(c, scheme, dt))) return r;
       if ((r = collect_timing(c, ns))) return r;
@@ -822,3 +834,5 @@ int pgpu_fp32_peak(int device, double *tflops, double *ms_out) {
 const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
 }  // extern "C"
+
+#include "surrogate_host.inc"

@@ -1,0 +1,328 @@
+// Surrogate evaluation on the octree of tree.cuh, FP32 with compensated sums.
+//
+// Far cells.  Beyond a few cell widths the Gaussian regularisation is below
+// FP32 resolution (tests/test_math_fits.py), so a far cell acts through the
+// singular kernel, written with phi(d) = 1/|d| (4 pi units, as the pair kernel):
+//   velocity    alpha_s x d / rho^3                     = -alpha_s x grad phi(d)
+//   stretching  b/rho^3 - 3 (d.b) d / rho^5, b = alpha_t x alpha_s  = -D2(d) b
+// Expanding d = r - y about the cell centroid (r = x_t - c, y = x_s - c) to
+// second order in y, with A = sum alpha, M_ab = sum alpha_a y_b,
+// Q_abc = sum alpha_a y_b y_c and Dn the n-th derivative tensors of phi at r:
+//   u_i = -eps_iab [A_a D1_b - M_ac D2_bc + 1/2 Q_acd D3_bcd]
+//   s_i = -[D2_ik B_k - D3_ikc N_kc + 1/2 D4_ikcd P_kcd],
+//         B = alpha_t x A, N_.c = alpha_t x M_.c, P_.cd = alpha_t x Q_.cd.
+// `order` 0 keeps the monopole, 1 adds the dipole, 2 the quadrupole.  The
+// contractions below never form D3/D4 (checked against full tensors in
+// tests/test_surrogate.py).
+//
+// Near leaves.  Exact pair sums with the same three-regime FP32 terms as the
+// direct kernel.
+#pragma once
+#include "kernels.cuh"
+#include "tree.cuh"
+
+namespace pgpu {
+
+__device__ __forceinline__ void cross3f(const float *a, const float *b, float *c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Velocity u and stretching s (4 pi units) induced at a target (position x,
+// strength at) by a far cell (data v), to the given order.
+__device__ __forceinline__ void far_expand(const float *v, const float *x, const float *at, int order, float *u,
+                                           float *s) {
+  const float r[3] = {x[0] - v[0], x[1] - v[1], x[2] - v[2]};
+  const float r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  const float ir = fast_rsqrt(r2);
+  const float ir2 = ir * ir, ir3 = ir * ir2, ir5 = ir3 * ir2, ir7 = ir5 * ir2, ir9 = ir7 * ir2;
+  const float A[3] = {v[3], v[4], v[5]};
+  float t[3];
+  cross3f(A, r, t);
+  for (int i = 0; i < 3; ++i) u[i] = ir3 * t[i];
+  float B[3];
+  cross3f(at, A, B);
+  const float rB = r[0] * B[0] + r[1] * B[1] + r[2] * B[2];
+  for (int i = 0; i < 3; ++i) s[i] = ir3 * B[i] - 3.f * ir5 * rB * r[i];
+  if (order < 1) return;
+  // ---- dipole
+  const float *M = v + 6;  // M[a*3+b]
+  float Mr[3];
+  for (int a = 0; a < 3; ++a) Mr[a] = M[3 * a] * r[0] + M[3 * a + 1] * r[1] + M[3 * a + 2] * r[2];
+  const float mx[3] = {M[5] - M[7], M[6] - M[2], M[1] - M[3]};
+  cross3f(Mr, r, t);
+  for (int i = 0; i < 3; ++i) u[i] += 3.f * ir5 * t[i] - ir3 * mx[i];
+  float N[3][3];  // N[k][c] = (at x M_.c)_k
+  for (int c = 0; c < 3; ++c) {
+    const float col[3] = {M[c], M[3 + c], M[6 + c]};
+    float n[3];
+    cross3f(at, col, n);
+    N[0][c] = n[0]; N[1][c] = n[1]; N[2][c] = n[2];
+  }
+  float Nr[3], NTr[3];
+  for (int i = 0; i < 3; ++i) {
+    Nr[i] = N[i][0] * r[0] + N[i][1] * r[1] + N[i][2] * r[2];
+    NTr[i] = N[0][i] * r[0] + N[1][i] * r[1] + N[2][i] * r[2];
+  }
+  const float rNr = r[0] * Nr[0] + r[1] * Nr[1] + r[2] * Nr[2];
+  const float trN = N[0][0] + N[1][1] + N[2][2];
+  for (int i = 0; i < 3; ++i) s[i] += -15.f * ir7 * rNr * r[i] + 3.f * ir5 * (Nr[i] + NTr[i] + r[i] * trN);
+  if (order < 2) return;
+  // ---- quadrupole; Q_a packed (00,01,02,11,12,22)
+  const float *Qp = v + 15;
+  float sv[3], tv[3], W[3][3];
+  for (int a = 0; a < 3; ++a) {
+    const float *q = Qp + 6 * a;
+    W[a][0] = q[0] * r[0] + q[1] * r[1] + q[2] * r[2];
+    W[a][1] = q[1] * r[0] + q[3] * r[1] + q[4] * r[2];
+    W[a][2] = q[2] * r[0] + q[4] * r[1] + q[5] * r[2];
+    sv[a] = r[0] * W[a][0] + r[1] * W[a][1] + r[2] * W[a][2];
+    tv[a] = q[0] + q[3] + q[5];
+  }
+  const float wx[3] = {W[1][2] - W[2][1], W[2][0] - W[0][2], W[0][1] - W[1][0]};
+  float sr[3], tr[3];
+  cross3f(sv, r, sr);
+  cross3f(tv, r, tr);
+  for (int i = 0; i < 3; ++i) u[i] += 7.5f * ir7 * sr[i] - 1.5f * ir5 * (2.f * wx[i] + tr[i]);
+  // P_k (symmetric over cd) = (at x Q_.cd)_k
+  float P[3][6];
+  for (int e = 0; e < 6; ++e) {
+    const float col[3] = {Qp[e], Qp[6 + e], Qp[12 + e]};
+    float p[3];
+    cross3f(at, col, p);
+    P[0][e] = p[0]; P[1][e] = p[1]; P[2][e] = p[2];
+  }
+  float Pr[3][3], rPr[3], trP[3];
+  for (int k = 0; k < 3; ++k) {
+    const float *q = P[k];
+    Pr[k][0] = q[0] * r[0] + q[1] * r[1] + q[2] * r[2];
+    Pr[k][1] = q[1] * r[0] + q[3] * r[1] + q[4] * r[2];
+    Pr[k][2] = q[2] * r[0] + q[4] * r[1] + q[5] * r[2];
+    rPr[k] = r[0] * Pr[k][0] + r[1] * Pr[k][1] + r[2] * Pr[k][2];
+    trP[k] = q[0] + q[3] + q[5];
+  }
+  const float srPr = r[0] * rPr[0] + r[1] * rPr[1] + r[2] * rPr[2];
+  const float sPrk = Pr[0][0] + Pr[1][1] + Pr[2][2];  // sum_k (P_k r)_k
+  const float rtr = r[0] * trP[0] + r[1] * trP[1] + r[2] * trP[2];
+  // sum_k P_k[i][k]: P_k packed; entry (i,k)
+  auto pik = [&](int k, int i) {
+    const int a = min(i, k), b = max(i, k);
+    const int e = a == 0 ? b : (a == 1 ? 2 + b : 5);
+    return P[k][e];
+  };
+  for (int i = 0; i < 3; ++i) {
+    const float sumPk = r[0] * Pr[0][i] + r[1] * Pr[1][i] + r[2] * Pr[2][i];
+    const float spik = pik(0, i) + pik(1, i) + pik(2, i);
+    const float d4p = 105.f * ir9 * r[i] * srPr -
+                      15.f * ir7 * (rPr[i] + 2.f * sumPk + 2.f * r[i] * sPrk + r[i] * rtr) +
+                      3.f * ir5 * (trP[i] + 2.f * spik);
+    s[i] -= 0.5f * d4p;
+  }
+}
+
+// One ordered pair with the FP32 three-regime terms of the direct kernel,
+// accumulated into CG-group partial sums.  Must be called by all lanes of a
+// warp together (it votes).
+__device__ __forceinline__ void pair_accum_f32(const float4 p, const float4 q, const float *xt, const float *at,
+                                               float hst, float h50, float vt, float *sv, float *sd, float *sp,
+                                               float *sdv) {
+  const float dx = xt[0] - p.x, dy = xt[1] - p.y, dz = xt[2] - p.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const bool near = fmaf(-kFarU, p.w, r2) < h50;
+  const float ir = fast_rsqrt(r2);
+  const float A = ir * ir;
+  float qq = A * ir, FF = -3.0f * qq * A, zd = 0.f;
+  bool diffuse = false;
+  if (__any_sync(0xffffffffu, near)) {
+    if (near) {
+      const PairTerms<float> pt = pair_terms_near(r2, hst + p.w);
+      qq = pt.q; FF = pt.F; zd = pt.zd;
+      diffuse = true;
+    }
+  }
+  const float wx = q.y * dz - q.z * dy, wy = q.z * dx - q.x * dz, wz = q.x * dy - q.y * dx;
+  sv[0] += qq * wx; sv[1] += qq * wy; sv[2] += qq * wz;
+  const float fd = FF * (at[0] * wx + at[1] * wy + at[2] * wz);
+  sd[0] += fd * dx; sd[1] += fd * dy; sd[2] += fd * dz;
+  sp[0] += qq * q.x; sp[1] += qq * q.y; sp[2] += qq * q.z;
+  if (diffuse) {
+    sdv[0] += zd * (vt * q.x - q.w * at[0]);
+    sdv[1] += zd * (vt * q.y - q.w * at[1]);
+    sdv[2] += zd * (vt * q.z - q.w * at[2]);
+  }
+}
+
+__device__ __forceinline__ void fold_group(const float *at, float nu2, float *sv, float *sd, float *sp, float *sdv,
+                                           float *vh, float *vl, float *dh, float *dl) {
+  const float e[3] = {at[1] * sp[2] - at[2] * sp[1] + sd[0] + nu2 * sdv[0],
+                      at[2] * sp[0] - at[0] * sp[2] + sd[1] + nu2 * sdv[1],
+                      at[0] * sp[1] - at[1] * sp[0] + sd[2] + nu2 * sdv[2]};
+  for (int m = 0; m < 3; ++m) {
+    two_sum_acc(vh[m], vl[m], sv[m]);
+    two_sum_acc(dh[m], dl[m], e[m]);
+    sv[m] = sd[m] = sp[m] = sdv[m] = 0.f;
+  }
+}
+
+struct TreeEvalArgs {
+  const CellData *cd;
+  const TreeCell *cells;
+  const int *leaves;
+  int nleaves;
+  const int *far_off, *far_cnt, *far_list;
+  const int *near_off, *near_cnt, *near_list;
+  const float4 *Ps, *Qs;  // sorted records
+  const int *idx;         // sorted position -> index within the system
+  int64_t off;            // slot offset of the system
+  double *partial;        // chunk 0 of [nch][6][cap]
+  int64_t cap;
+  float nu2;
+  int order;
+};
+
+constexpr int kTreeBlock = 256;
+constexpr int kTreeTPT = 2;  // leaves hold at most 512 particles
+constexpr int kFarChunk = 32;
+
+__global__ void __launch_bounds__(kTreeBlock) tree_eval_kernel(TreeEvalArgs a) {
+  __shared__ float sc[kFarChunk][kCellFloats];
+  __shared__ float4 sP[kTreeBlock], sQ[kTreeBlock];
+  const int tid = threadIdx.x;
+  for (int li = blockIdx.x; li < a.nleaves; li += gridDim.x) {
+    const TreeCell tc = a.cells[a.leaves[li]];
+    float xt[kTreeTPT][3], at[kTreeTPT][3], hst[kTreeTPT], h50[kTreeTPT], vt[kTreeTPT];
+    float vh[kTreeTPT][3], vl[kTreeTPT][3], dh[kTreeTPT][3], dl[kTreeTPT][3];
+    for (int k = 0; k < kTreeTPT; ++k) {
+      const int t = min(tc.start + tid + k * kTreeBlock, tc.end - 1);
+      const float4 p = a.Ps[t], q = a.Qs[t];
+      xt[k][0] = p.x; xt[k][1] = p.y; xt[k][2] = p.z; hst[k] = p.w; h50[k] = kFarU * p.w;
+      at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
+      for (int m = 0; m < 3; ++m) vh[k][m] = vl[k][m] = dh[k][m] = dl[k][m] = 0.f;
+    }
+    // ---- far cells, in chunks staged in shared memory
+    const int fo = a.far_off[li], fn = a.far_cnt[li];
+    for (int c0 = 0; c0 < fn; c0 += kFarChunk) {
+      const int cn = min(kFarChunk, fn - c0);
+      __syncthreads();
+      for (int e = tid; e < cn * kCellFloats; e += kTreeBlock)
+        sc[e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
+      __syncthreads();
+      for (int k = 0; k < kTreeTPT; ++k) {
+        float su[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
+        for (int j = 0; j < cn; ++j) {
+          float u[3], s[3];
+          far_expand(sc[j], xt[k], at[k], a.order, u, s);
+          for (int m = 0; m < 3; ++m) { su[m] += u[m]; ss[m] += s[m]; }
+        }
+        for (int m = 0; m < 3; ++m) {
+          two_sum_acc(vh[k][m], vl[k][m], su[m]);
+          two_sum_acc(dh[k][m], dl[k][m], ss[m]);
+        }
+      }
+    }
+    // ---- near leaves, exact
+    const int no = a.near_off[li], nn = a.near_cnt[li];
+    for (int ni = 0; ni < nn; ++ni) {
+      const TreeCell sc_ = a.cells[a.near_list[no + ni]];
+      for (int sb = sc_.start; sb < sc_.end; sb += kTreeBlock) {
+        __syncthreads();
+        const int j = sb + tid;
+        if (j < sc_.end) { sP[tid] = a.Ps[j]; sQ[tid] = a.Qs[j]; }
+        else { sP[tid] = pad_P<float>(); sQ[tid] = pad_Q<float>(); }
+        __syncthreads();
+        const int cnt = min(kTreeBlock, sc_.end - sb);
+        for (int g = 0; g < cnt; g += 32) {
+          float sv[kTreeTPT][3] = {}, sd[kTreeTPT][3] = {}, sp[kTreeTPT][3] = {}, sdv[kTreeTPT][3] = {};
+          const int gn = min(32, cnt - g);
+          for (int jj = 0; jj < gn; ++jj) {
+            const float4 p = sP[g + jj], q = sQ[g + jj];
+#pragma unroll
+            for (int k = 0; k < kTreeTPT; ++k)
+              pair_accum_f32(p, q, xt[k], at[k], hst[k], h50[k], vt[k], sv[k], sd[k], sp[k], sdv[k]);
+          }
+#pragma unroll
+          for (int k = 0; k < kTreeTPT; ++k)
+            fold_group(at[k], a.nu2, sv[k], sd[k], sp[k], sdv[k], vh[k], vl[k], dh[k], dl[k]);
+        }
+      }
+    }
+    for (int k = 0; k < kTreeTPT; ++k) {
+      const int t = tc.start + tid + k * kTreeBlock;
+      if (t < tc.end) {
+        double *o = a.partial + a.off + a.idx[t];
+        for (int m = 0; m < 3; ++m) {
+          o[m * a.cap] = ((double)vh[k][m] + (double)vl[k][m]) * kInv4Pi;
+          o[(3 + m) * a.cap] = ((double)dh[k][m] + (double)dl[k][m]) * kInv4Pi;
+        }
+      }
+    }
+  }
+}
+
+// Exact rates (direct FP32C sum over all n particles of the system) at nt
+// sampled targets, split over gridDim.y source chunks:
+// out[c][m][t], m = 0..5.
+__global__ void __launch_bounds__(kTreeBlock) sample_exact_kernel(const float4 *P, const float4 *Q, int64_t off,
+                                                                  int64_t n, const int *targets, int nt, float nu2,
+                                                                  double *out) {
+  __shared__ float4 sP[kTreeBlock], sQ[kTreeBlock];
+  const int tid = threadIdx.x;
+  const int ti = blockIdx.x * kTreeBlock + tid;
+  const int64_t t = off + targets[min(ti, nt - 1)];
+  const float4 pt = P[t], qt = Q[t];
+  const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
+  const float hst = pt.w, h50 = kFarU * pt.w, vt = qt.w;
+  float vh[3] = {0, 0, 0}, vl[3] = {0, 0, 0}, dh[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+  const int64_t per = (n + gridDim.y - 1) / gridDim.y;
+  const int64_t s0 = off + blockIdx.y * per, s1 = min(off + n, s0 + per);
+  for (int64_t sb = s0; sb < s1; sb += kTreeBlock) {
+    __syncthreads();
+    const int64_t j = sb + tid;
+    if (j < s1) { sP[tid] = P[j]; sQ[tid] = Q[j]; }
+    else { sP[tid] = pad_P<float>(); sQ[tid] = pad_Q<float>(); }
+    __syncthreads();
+    for (int g = 0; g < kTreeBlock; g += 32) {
+      float sv[3] = {}, sd[3] = {}, sp[3] = {}, sdv[3] = {};
+      for (int jj = 0; jj < 32; ++jj) pair_accum_f32(sP[g + jj], sQ[g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
+      fold_group(at, nu2, sv, sd, sp, sdv, vh, vl, dh, dl);
+    }
+  }
+  if (ti < nt) {
+    double *o = out + (int64_t)blockIdx.y * 6 * nt + ti;
+    for (int m = 0; m < 3; ++m) {
+      o[m * nt] = ((double)vh[m] + (double)vl[m]) * kInv4Pi;
+      o[(3 + m) * nt] = ((double)dh[m] + (double)dl[m]) * kInv4Pi;
+    }
+  }
+}
+
+// Max-norm errors of the surrogate rates (chunk 0 of partial) at the sampled
+// targets against the exact sums: res[0] = max |dv|^2, res[1] = max |v|^2,
+// res[2] = max |d dalpha|^2, res[3] = max |dalpha|^2 (ordered-float atomics).
+__global__ void sample_compare_kernel(const double *exact, int chunks, int nt, const int *targets, int64_t off,
+                                      const double *partial, int64_t cap, unsigned *res) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double ex[6];
+  for (int m = 0; m < 6; ++m) {
+    double v = 0;
+    for (int c = 0; c < chunks; ++c) v += exact[((int64_t)c * 6 + m) * nt + t];
+    ex[m] = v;
+  }
+  const int64_t i = off + targets[t];
+  double dv = 0, v2 = 0, da = 0, a2 = 0;
+  for (int m = 0; m < 3; ++m) {
+    const double s = partial[m * cap + i], sa = partial[(3 + m) * cap + i];
+    dv += (s - ex[m]) * (s - ex[m]);
+    v2 += ex[m] * ex[m];
+    da += (sa - ex[3 + m]) * (sa - ex[3 + m]);
+    a2 += ex[3 + m] * ex[3 + m];
+  }
+  atomicMax(&res[0], f2ord((float)dv));
+  atomicMax(&res[1], f2ord((float)v2));
+  atomicMax(&res[2], f2ord((float)da));
+  atomicMax(&res[3], f2ord((float)a2));
+}
+
+}  // namespace pgpu

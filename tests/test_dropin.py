@@ -23,10 +23,7 @@ DRIVER = ROOT / "tests" / "_build" / "dropin_check"
 @pytest.fixture(scope="module")
 def driver():
     if not DRIVER.exists():
-        if not Path("/root/reference").exists():
-            pytest.skip("drop-in driver not built and PAWAN sources absent")
-        env = {k: v for k, v in os.environ.items() if k not in ("CXX", "CC")}
-        subprocess.run(["make", "-C", str(ROOT / "tests" / "dropin")], check=True, env=env, capture_output=True)
+        pytest.skip("drop-in driver not built (make -C tests/dropin PAWAN_SRC=<PAWAN tree>)")
     return DRIVER
 
 

@@ -1,0 +1,108 @@
+"""Far-field surrogate: octree near field (exact) + multipole far field, with
+the sampled-target gate that reverts to the direct sum."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pawan_b200 import capi, cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rings():
+    return cases.leapfrog_rings(n_total=200_000)
+
+
+def direct(w, nu=1e-4):
+    c = capi.Context(precision=capi.FP32C, nu=nu)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    c.solve()
+    v, a = c.rates(k)
+    c.close()
+    return v, a
+
+
+def surrogate(w, nu=1e-4, **kw):
+    c = capi.Context(precision=capi.FP32C, nu=nu)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    c.surrogate_enable(**kw)
+    c.solve()
+    v, a = c.rates(k)
+    st = c.surrogate_stats()
+    c.close()
+    return v, a, st
+
+
+def test_all_near_equals_direct(gpu, rings):
+    """With a near field covering everything, every source is summed exactly
+    once through the leaves: the result is the direct sum."""
+    vd, ad = direct(rings)
+    v, a, st = surrogate(rings, near_widths=1e9, check_targets=0)
+    assert st["far_entries"] == 0 and st["leaves"] > 100
+    assert O.rel_err(v, vd) < 2e-6
+    assert O.rel_err(a, ad) < 2e-6
+
+
+def test_orders_converge_and_quadrupole_meets_gate(gpu, rings):
+    vd, ad = direct(rings)
+    errs = []
+    for order in (0, 1, 2):
+        v, a, st = surrogate(rings, order=order, check_targets=0)
+        errs.append(O.rel_err(v, vd))
+        assert st["fallbacks"] == 0
+    assert errs[2] < errs[0]
+    assert errs[2] < 1e-4, errs
+
+
+def test_sampled_gate_reports_error(gpu, rings):
+    vd, ad = direct(rings)
+    v, a, st = surrogate(rings, order=2, tolerance=1.0)
+    full = O.rel_err(v, vd)
+    assert st["evaluations"] == 1 and st["fallbacks"] == 0
+    # the sampled estimate is a lower bound of the full max-norm error, of the same size
+    assert st["last_err_vel"] <= full * 1.0001 + 1e-12
+    assert st["last_err_vel"] > 0.05 * full
+
+
+def test_gate_reverts_to_direct_sum(gpu, rings):
+    vd, ad = direct(rings)
+    v, a, st = surrogate(rings, order=0, tolerance=1e-12)
+    assert st["fallbacks"] == 1
+    assert O.rel_err(v, vd) < 2e-6 and O.rel_err(a, ad) < 2e-6
+
+
+def test_surrogate_rk4_steps_track_direct(gpu):
+    w = cases.leapfrog_rings(n_total=100_000)
+    out = []
+    for sur in (False, True):
+        c = capi.Context(precision=capi.FP32C, nu=1e-4)
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        if sur:
+            c.surrogate_enable(order=2)
+        c.step("rk4", 0.005, 2)
+        out.append(c.state(k))
+        if sur:
+            assert c.surrogate_stats()["evaluations"] == 8
+        c.close()
+    assert O.rel_err(out[1][0] - w.pos, out[0][0] - w.pos) < 1e-4
+    assert O.rel_err(out[1][1], out[0][1]) < 1e-4
+
+
+def test_surrogate_host_errors(gpu):
+    w = cases.ring_stations(stations=40)
+    c = capi.Context(precision=capi.FP64, nu=1e-4)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    with pytest.raises(capi.PgpuError):
+        c.surrogate_enable()
+    c3 = capi.Context(precision=capi.FP32C, nu=1e-4)
+    a = c3.add_wake(w.n, system=0)
+    b = c3.add_wake(w.n, system=1)
+    c3.set_particles(a, w)
+    c3.set_particles(b, w)
+    with pytest.raises(capi.PgpuError):
+        c3.surrogate_enable()
