@@ -188,6 +188,13 @@ void pgpu_surrogate_config_default(pgpu_surrogate_config *cfg);
 int pgpu_surrogate_enable(pgpu_ctx *ctx, int32_t system, const pgpu_surrogate_config *cfg);
 int pgpu_surrogate_disable(pgpu_ctx *ctx);
 int pgpu_surrogate_get_stats(pgpu_ctx *ctx, pgpu_surrogate_stats *stats);
+/* Copies the octree of the last surrogate evaluation to host buffers (for
+ * inspection and tests): idx[n] maps sorted position to particle index;
+ * cell[4 ncells] = (start, end, first_child, nchild) per cell; leaves[nleaves]
+ * are cell indices; counts[2 nleaves] = far- then near-list lengths.  Any
+ * buffer may be NULL; a buffer smaller than needed is left untouched. */
+int pgpu_surrogate_tree(pgpu_ctx *ctx, int *idx, int64_t idx_cap, int *cell, int64_t cell_cap, int *leaves,
+                        int *counts, int64_t leaf_cap, int64_t *n, int64_t *ncells, int64_t *nleaves);
 
 /* The context's CUDA stream (a cudaStream_t), so a caller can order its own
  * work or timing events with the library's launches.  No PAWAN counterpart. */

@@ -33,7 +33,7 @@ EXPORTS = [
     "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
     "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
     "pgpu_fp32_peak", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
-    "pgpu_surrogate_disable", "pgpu_surrogate_get_stats",
+    "pgpu_surrogate_disable", "pgpu_surrogate_get_stats", "pgpu_surrogate_tree",
 ]
 
 
@@ -117,6 +117,8 @@ def load(build_if_missing: bool = False):
         "pgpu_surrogate_enable": (C.c_int, [vp, C.c_int32, C.POINTER(SurrogateConfig)]),
         "pgpu_surrogate_disable": (C.c_int, [vp]),
         "pgpu_surrogate_get_stats": (C.c_int, [vp, C.POINTER(SurrogateStats)]),
+        "pgpu_surrogate_tree": (C.c_int, [vp, C.POINTER(C.c_int), C.c_int64, C.POINTER(C.c_int), C.c_int64,
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int64, _i64p, _i64p, _i64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -287,6 +289,21 @@ class Context:
         st = SurrogateStats()
         self._ck(self.lib.pgpu_surrogate_get_stats(self.h, C.byref(st)))
         return st.as_dict()
+
+    def surrogate_tree(self) -> dict:
+        """Octree of the last surrogate evaluation (host copies)."""
+        n, nc, nl = C.c_int64(), C.c_int64(), C.c_int64()
+        ip = C.POINTER(C.c_int)
+        self._ck(self.lib.pgpu_surrogate_tree(self.h, None, 0, None, 0, None, None, 0, C.byref(n), C.byref(nc),
+                                              C.byref(nl)))
+        idx = np.zeros(n.value, np.int32)
+        cell = np.zeros((nc.value, 4), np.int32)
+        leaves = np.zeros(nl.value, np.int32)
+        counts = np.zeros((2, nl.value), np.int32)
+        self._ck(self.lib.pgpu_surrogate_tree(self.h, idx.ctypes.data_as(ip), n.value, cell.ctypes.data_as(ip),
+                                              nc.value, leaves.ctypes.data_as(ip), counts.ctypes.data_as(ip),
+                                              nl.value, C.byref(n), C.byref(nc), C.byref(nl)))
+        return {"idx": idx, "cells": cell, "leaves": leaves, "far": counts[0], "near": counts[1]}
 
     def launch_count(self) -> int:
         return int(self.lib.pgpu_launch_count(self.h))

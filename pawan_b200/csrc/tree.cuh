@@ -136,7 +136,7 @@ __global__ void split_count_kernel(TreeCell *cells, int f0, int f1, const unsign
     const int shift = 3 * (kTreeLevels - c.level - 1);
     int lo = c.start;
     for (int o = 0; o < 8; ++o) {
-      const int hi = lower_bound_prefix(code, lo, c.end, shift, (c.prefix << 3) | (unsigned long long)(o + 1));
+      const int hi = lower_bound_prefix(code, lo, c.end, shift, (c.prefix << 3) + (unsigned long long)(o + 1));
       k += hi > lo;
       lo = hi;
     }
@@ -158,7 +158,7 @@ __global__ void split_write_kernel(TreeCell *cells, int f0, int f1, const unsign
   const int shift = 3 * (kTreeLevels - c.level - 1);
   int lo = c.start, w = base + offs[i - f0], k = 0;
   for (int o = 0; o < 8; ++o) {
-    const int hi = lower_bound_prefix(code, lo, c.end, shift, (c.prefix << 3) | (unsigned long long)(o + 1));
+    const int hi = lower_bound_prefix(code, lo, c.end, shift, (c.prefix << 3) + (unsigned long long)(o + 1));
     if (hi > lo) {
       TreeCell ch;
       ch.start = lo; ch.end = hi; ch.first_child = -1; ch.nchild = 0; ch.level = c.level + 1; ch.pad = 0;

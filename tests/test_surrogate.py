@@ -106,3 +106,25 @@ def test_surrogate_host_errors(gpu):
     c3.set_particles(b, w)
     with pytest.raises(capi.PgpuError):
         c3.surrogate_enable()
+
+
+def test_octree_partitions_particles(gpu):
+    w = cases.leapfrog_rings(n_total=50_000)
+    c = capi.Context(precision=capi.FP32C, nu=1e-4)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    c.surrogate_enable(check_targets=0, leaf_size=64)
+    c.solve()
+    t = c.surrogate_tree()
+    assert np.array_equal(np.sort(t["idx"]), np.arange(w.n))
+    cells = t["cells"]
+    assert cells[0, 0] == 0 and cells[0, 1] == w.n
+    for i, (s0, s1, fc, nc) in enumerate(cells):
+        if nc:
+            ch = cells[fc:fc + nc]
+            assert ch[0, 0] == s0 and ch[-1, 1] == s1 and np.all(ch[1:, 0] == ch[:-1, 1])
+    lv = cells[t["leaves"]]
+    assert np.all(cells[t["leaves"], 3] == 0)
+    order = np.argsort(lv[:, 0])
+    assert lv[order[0], 0] == 0 and lv[order[-1], 1] == w.n and np.all(lv[order][1:, 0] == lv[order][:-1, 1])
+    assert np.all(lv[:, 1] - lv[:, 0] <= 64)
