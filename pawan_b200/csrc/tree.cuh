@@ -251,12 +251,15 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
 }
 
 // Interaction lists of every leaf (one thread per leaf).  pass 0 counts,
-// pass 1 writes at the offsets of an exclusive scan of the counts.  The
-// stack is bounded (kListStack); overflow sets *err and truncates nothing
-// silently: the caller treats a non-zero *err as a failed build.
+// pass 1 writes at the offsets of an exclusive scan of the counts.  Near
+// leaves are emitted as runs of the sorted particle order: consecutive near
+// leaves whose ranges touch are merged (siblings are visited in octant order,
+// which is sorted order, so runs are long).  The stack is bounded
+// (kListStack); overflow sets *err, and the caller treats a non-zero *err as a
+// failed build.
 __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const int *leaves, int nleaves,
                              float near_widths, int pass, int *far_cnt, int *near_cnt, const int *far_off,
-                             const int *near_off, int *far_list, int *near_list, int *err) {
+                             const int *near_off, int *far_list, int2 *near_runs, int *err) {
   const int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= nleaves) return;
   const int T = leaves[li];
@@ -265,8 +268,8 @@ __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const in
   int stack[kListStack];
   int sp = 0;
   stack[sp++] = 0;
-  int nf = 0, nn = 0;
-  int fo = pass ? far_off[li] : 0, no = pass ? near_off[li] : 0;
+  int nf = 0, nn = 0, run_s = -1, run_e = -1;
+  const int fo = pass ? far_off[li] : 0, no = pass ? near_off[li] : 0;
   while (sp > 0) {
     const int ci = stack[--sp];
     const TreeCell c = cells[ci];
@@ -277,15 +280,28 @@ __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const in
       if (pass) far_list[fo + nf] = ci;
       ++nf;
     } else if (c.nchild == 0) {
-      if (pass) near_list[no + nn] = ci;
-      ++nn;
+      if (c.start == run_e) {
+        run_e = c.end;
+      } else {
+        if (run_s >= 0) {
+          if (pass) near_runs[no + nn] = make_int2(run_s, run_e);
+          ++nn;
+        }
+        run_s = c.start;
+        run_e = c.end;
+      }
     } else {
       if (sp + c.nchild > kListStack) {
         atomicExch(err, 1);
         break;
       }
-      for (int k = 0; k < c.nchild; ++k) stack[sp++] = c.first_child + k;
+      // push in reverse so the children are visited in octant (sorted) order
+      for (int k = c.nchild - 1; k >= 0; --k) stack[sp++] = c.first_child + k;
     }
+  }
+  if (run_s >= 0) {
+    if (pass) near_runs[no + nn] = make_int2(run_s, run_e);
+    ++nn;
   }
   if (!pass) {
     far_cnt[li] = nf;

@@ -12,8 +12,9 @@
 //   s_i = -[D2_ik B_k - D3_ikc N_kc + 1/2 D4_ikcd P_kcd],
 //         B = alpha_t x A, N_.c = alpha_t x M_.c, P_.cd = alpha_t x Q_.cd.
 // `order` 0 keeps the monopole, 1 adds the dipole, 2 the quadrupole.  The
-// contractions below never form D3/D4 (checked against full tensors in
-// tests/test_surrogate.py).
+// contractions below never form D3/D4; tests/test_surrogate.py checks the
+// result end to end (the order-2 far field reproduces the direct sum to
+// ~2e-5 on the leapfrogging rings, and the error falls with the order).
 //
 // Near leaves.  Exact pair sums with the same three-regime FP32 terms as the
 // direct kernel.
@@ -171,7 +172,8 @@ struct TreeEvalArgs {
   const int *leaves;
   int nleaves;
   const int *far_off, *far_cnt, *far_list;
-  const int *near_off, *near_cnt, *near_list;
+  const int *near_off, *near_cnt;
+  const int2 *near_runs;  // sorted-order particle ranges of the near field
   const float4 *Ps, *Qs;  // sorted records
   const int *idx;         // sorted position -> index within the system
   int64_t off;            // slot offset of the system
@@ -181,80 +183,70 @@ struct TreeEvalArgs {
   int order;
 };
 
-constexpr int kTreeBlock = 256;
-constexpr int kTreeTPT = 2;  // leaves hold at most 512 particles
+constexpr int kTreeBlock = 256;  // sampled-check kernel
+constexpr int kLeafBlock = 512;  // one thread per target of a leaf (leaves hold <= 512)
 constexpr int kFarChunk = 32;
 
-__global__ void __launch_bounds__(kTreeBlock) tree_eval_kernel(TreeEvalArgs a) {
+// One CTA per target leaf, one thread per target.  Warps past the end of the
+// leaf only help stage shared memory; they issue no arithmetic.
+__global__ void __launch_bounds__(kLeafBlock) tree_eval_kernel(TreeEvalArgs a) {
   __shared__ float sc[kFarChunk][kCellFloats];
-  __shared__ float4 sP[kTreeBlock], sQ[kTreeBlock];
+  __shared__ float4 sP[kLeafBlock], sQ[kLeafBlock];
   const int tid = threadIdx.x;
   for (int li = blockIdx.x; li < a.nleaves; li += gridDim.x) {
     const TreeCell tc = a.cells[a.leaves[li]];
-    float xt[kTreeTPT][3], at[kTreeTPT][3], hst[kTreeTPT], h50[kTreeTPT], vt[kTreeTPT];
-    float vh[kTreeTPT][3], vl[kTreeTPT][3], dh[kTreeTPT][3], dl[kTreeTPT][3];
-    for (int k = 0; k < kTreeTPT; ++k) {
-      const int t = min(tc.start + tid + k * kTreeBlock, tc.end - 1);
-      const float4 p = a.Ps[t], q = a.Qs[t];
-      xt[k][0] = p.x; xt[k][1] = p.y; xt[k][2] = p.z; hst[k] = p.w; h50[k] = kFarU * p.w;
-      at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
-      for (int m = 0; m < 3; ++m) vh[k][m] = vl[k][m] = dh[k][m] = dl[k][m] = 0.f;
-    }
+    const bool active = tc.start + (tid & ~31) < tc.end;  // warp-uniform
+    const int t = min(tc.start + tid, tc.end - 1);
+    const float4 pt = a.Ps[t], qt = a.Qs[t];
+    const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
+    const float hst = pt.w, h50 = kFarU * pt.w, vt = qt.w;
+    float vh[3] = {0, 0, 0}, vl[3] = {0, 0, 0}, dh[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
     // ---- far cells, in chunks staged in shared memory
     const int fo = a.far_off[li], fn = a.far_cnt[li];
     for (int c0 = 0; c0 < fn; c0 += kFarChunk) {
       const int cn = min(kFarChunk, fn - c0);
       __syncthreads();
-      for (int e = tid; e < cn * kCellFloats; e += kTreeBlock)
+      for (int e = tid; e < cn * kCellFloats; e += kLeafBlock)
         sc[e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
       __syncthreads();
-      for (int k = 0; k < kTreeTPT; ++k) {
+      if (active) {
         float su[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
         for (int j = 0; j < cn; ++j) {
           float u[3], s[3];
-          far_expand(sc[j], xt[k], at[k], a.order, u, s);
+          far_expand(sc[j], xt, at, a.order, u, s);
           for (int m = 0; m < 3; ++m) { su[m] += u[m]; ss[m] += s[m]; }
         }
         for (int m = 0; m < 3; ++m) {
-          two_sum_acc(vh[k][m], vl[k][m], su[m]);
-          two_sum_acc(dh[k][m], dl[k][m], ss[m]);
+          two_sum_acc(vh[m], vl[m], su[m]);
+          two_sum_acc(dh[m], dl[m], ss[m]);
         }
       }
     }
-    // ---- near leaves, exact
+    // ---- near field, exact, over sorted-order runs in tiles of kLeafBlock records
     const int no = a.near_off[li], nn = a.near_cnt[li];
     for (int ni = 0; ni < nn; ++ni) {
-      const TreeCell sc_ = a.cells[a.near_list[no + ni]];
-      for (int sb = sc_.start; sb < sc_.end; sb += kTreeBlock) {
+      const int2 run = a.near_runs[no + ni];
+      for (int sb = run.x; sb < run.y; sb += kLeafBlock) {
         __syncthreads();
         const int j = sb + tid;
-        if (j < sc_.end) { sP[tid] = a.Ps[j]; sQ[tid] = a.Qs[j]; }
-        else { sP[tid] = pad_P<float>(); sQ[tid] = pad_Q<float>(); }
+        if (j < run.y) { sP[tid] = a.Ps[j]; sQ[tid] = a.Qs[j]; }
         __syncthreads();
-        const int cnt = min(kTreeBlock, sc_.end - sb);
-        for (int g = 0; g < cnt; g += 32) {
-          float sv[kTreeTPT][3] = {}, sd[kTreeTPT][3] = {}, sp[kTreeTPT][3] = {}, sdv[kTreeTPT][3] = {};
-          const int gn = min(32, cnt - g);
-          for (int jj = 0; jj < gn; ++jj) {
-            const float4 p = sP[g + jj], q = sQ[g + jj];
-#pragma unroll
-            for (int k = 0; k < kTreeTPT; ++k)
-              pair_accum_f32(p, q, xt[k], at[k], hst[k], h50[k], vt[k], sv[k], sd[k], sp[k], sdv[k]);
+        if (active) {
+          const int cnt = min(kLeafBlock, run.y - sb);
+          for (int g = 0; g < cnt; g += 32) {
+            float sv[3] = {}, sd[3] = {}, sp[3] = {}, sdv[3] = {};
+            const int gn = min(32, cnt - g);
+            for (int jj = 0; jj < gn; ++jj) pair_accum_f32(sP[g + jj], sQ[g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
+            fold_group(at, a.nu2, sv, sd, sp, sdv, vh, vl, dh, dl);
           }
-#pragma unroll
-          for (int k = 0; k < kTreeTPT; ++k)
-            fold_group(at[k], a.nu2, sv[k], sd[k], sp[k], sdv[k], vh[k], vl[k], dh[k], dl[k]);
         }
       }
     }
-    for (int k = 0; k < kTreeTPT; ++k) {
-      const int t = tc.start + tid + k * kTreeBlock;
-      if (t < tc.end) {
-        double *o = a.partial + a.off + a.idx[t];
-        for (int m = 0; m < 3; ++m) {
-          o[m * a.cap] = ((double)vh[k][m] + (double)vl[k][m]) * kInv4Pi;
-          o[(3 + m) * a.cap] = ((double)dh[k][m] + (double)dl[k][m]) * kInv4Pi;
-        }
+    if (tc.start + tid < tc.end) {
+      double *o = a.partial + a.off + a.idx[tc.start + tid];
+      for (int m = 0; m < 3; ++m) {
+        o[m * a.cap] = ((double)vh[m] + (double)vl[m]) * kInv4Pi;
+        o[(3 + m) * a.cap] = ((double)dh[m] + (double)dl[m]) * kInv4Pi;
       }
     }
   }
