@@ -252,6 +252,97 @@ __global__ void __launch_bounds__(kLeafBlock) tree_eval_kernel(TreeEvalArgs a) {
   }
 }
 
+// Warp-independent form: every warp takes work items (target leaf, slice of
+// 32 of its targets) from an atomic counter and stages its own source tiles,
+// synchronising only within the warp.  Leaves average ~130 particles, so
+// whole-leaf CTAs leave most warps idle; independent warps keep ~48 warps per
+// SM busy.  items[k] = (leaf index, slice); counter[0] must be 0 at launch.
+constexpr int kWarpTile = 64;
+constexpr int kWarpCells = 16;
+constexpr int kWarpsPerCta = 4;
+
+__global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeEvalArgs a, const int2 *items,
+                                                                         int nitems, unsigned *counter) {
+  __shared__ float sc[kWarpsPerCta][kWarpCells][kCellFloats];
+  __shared__ float4 sP[kWarpsPerCta][kWarpTile], sQ[kWarpsPerCta][kWarpTile];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(counter, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int2 it = items[item];
+    const int li = it.x;
+    const TreeCell tc = a.cells[a.leaves[li]];
+    const int t0 = tc.start + it.y * 32 + lane;
+    const int t = min(t0, tc.end - 1);
+    const float4 pt = a.Ps[t], qt = a.Qs[t];
+    const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
+    const float hst = pt.w, h50 = kFarU * pt.w, vt = qt.w;
+    float vh[3] = {0, 0, 0}, vl[3] = {0, 0, 0}, dh[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+    const int fo = a.far_off[li], fn = a.far_cnt[li];
+    for (int c0 = 0; c0 < fn; c0 += kWarpCells) {
+      const int cn = min(kWarpCells, fn - c0);
+      __syncwarp();
+      for (int e = lane; e < cn * kCellFloats; e += 32)
+        sc[w][e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
+      __syncwarp();
+      float su[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
+      for (int j = 0; j < cn; ++j) {
+        float u[3], s[3];
+        far_expand(sc[w][j], xt, at, a.order, u, s);
+        for (int m = 0; m < 3; ++m) { su[m] += u[m]; ss[m] += s[m]; }
+      }
+      for (int m = 0; m < 3; ++m) {
+        two_sum_acc(vh[m], vl[m], su[m]);
+        two_sum_acc(dh[m], dl[m], ss[m]);
+      }
+    }
+    const int no = a.near_off[li], nn = a.near_cnt[li];
+    for (int ni = 0; ni < nn; ++ni) {
+      const int2 run = a.near_runs[no + ni];
+      for (int sb = run.x; sb < run.y; sb += kWarpTile) {
+        __syncwarp();
+        for (int k = lane; k < kWarpTile; k += 32) {
+          const int j = sb + k;
+          if (j < run.y) { sP[w][k] = a.Ps[j]; sQ[w][k] = a.Qs[j]; }
+        }
+        __syncwarp();
+        const int cnt = min(kWarpTile, run.y - sb);
+        for (int g = 0; g < cnt; g += 32) {
+          float sv[3] = {}, sd[3] = {}, sp[3] = {}, sdv[3] = {};
+          const int gn = min(32, cnt - g);
+          for (int jj = 0; jj < gn; ++jj)
+            pair_accum_f32(sP[w][g + jj], sQ[w][g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
+          fold_group(at, a.nu2, sv, sd, sp, sdv, vh, vl, dh, dl);
+        }
+      }
+    }
+    if (t0 < tc.end) {
+      double *o = a.partial + a.off + a.idx[t0];
+      for (int m = 0; m < 3; ++m) {
+        o[m * a.cap] = ((double)vh[m] + (double)vl[m]) * kInv4Pi;
+        o[(3 + m) * a.cap] = ((double)dh[m] + (double)dl[m]) * kInv4Pi;
+      }
+    }
+  }
+}
+
+// (leaf, slice) work items: count[li] = ceil(size / 32), then written at the
+// exclusive-scan offsets.
+__global__ void slice_count_kernel(const TreeCell *cells, const int *leaves, int nleaves, int *cnt) {
+  const int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li < nleaves) {
+    const TreeCell c = cells[leaves[li]];
+    cnt[li] = (c.end - c.start + 31) / 32;
+  }
+}
+__global__ void slice_write_kernel(const int *cnt, const int *off, int nleaves, int2 *items) {
+  const int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li < nleaves)
+    for (int k = 0; k < cnt[li]; ++k) items[off[li] + k] = make_int2(li, k);
+}
+
 // Exact rates (direct FP32C sum over all n particles of the system) at nt
 // sampled targets, split over gridDim.y source chunks:
 // out[c][m][t], m = 0..5.
