@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--stations", type=int, default=N_STATIONS, help="smaller rings for quick checks")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--surrogate-n", type=int, default=4_000_000)
     return ap.parse_args()
 
 
@@ -169,6 +171,51 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------------------ surrogate
+def run_surrogate(args, device: int) -> dict:
+    """Two coaxial leapfrogging rings (R = 1 and 1.2, Gamma = 1, a = 0.1,
+    sigma = 0.02, seed 4): one RK4 step with the octree far field (quadrupole,
+    near field within 4 cell widths exact, 4096 sampled targets re-checked
+    against the direct sum every evaluation) against the plain direct sum.  The
+    direct RK4 step is timed as four rate evaluations (its stage updates are
+    ~1e-4 of it); the surrogate step is timed whole."""
+    import torch
+    from pawan_b200 import capi, cases
+    w = cases.leapfrog_rings(n_total=args.surrogate_n)
+    out = {"workload": f"two coaxial rings N={w.n} (R=1, 1.2, Gamma=1, a=0.1, sigma=0.02, dz=0.3, seed 4), RK4 dt={DT}"}
+    c = capi.Context(precision=capi.FP32C, nu=NU, device=device)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    c.solve()
+    c.sync()
+    c.pair_kernel_time()
+    c.solve()
+    c.sync()
+    direct_eval_ms, _ = c.pair_kernel_time()
+    c.surrogate_enable(order=2, tolerance=1e-4, check_targets=4096)
+    c.solve()  # warm-up (tree buffers)
+    c.sync()
+    stream = torch.cuda.ExternalStream(c.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    c.step("rk4", DT, 1)
+    e1.record(stream)
+    e1.synchronize()
+    st = c.surrogate_stats()
+    sur_ms = e0.elapsed_time(e1)
+    direct_step_ms = 4 * direct_eval_ms
+    out.update({"direct_eval_ms": direct_eval_ms, "direct_step_ms": direct_step_ms, "surrogate_step_ms": sur_ms,
+                "surrogate_steps_per_s": 1e3 / sur_ms, "direct_steps_per_s": 1e3 / direct_step_ms,
+                "speedup": direct_step_ms / sur_ms, "sampled_rel_err_vel_max": st["max_err_vel"],
+                "sampled_rel_err_dalpha_last": st["last_err_dalpha"], "fallbacks": st["fallbacks"],
+                "evaluations": st["evaluations"], "far_order": 2, "learned_correction": False,
+                "tree": {"cells": st["cells"], "leaves": st["leaves"], "far_entries": st["far_entries"],
+                         "near_runs": st["near_entries"]},
+                "phase_ms_last_eval": {"tree": st["ms_tree"], "eval": st["ms_eval"], "check": st["ms_check"]}})
+    c.close()
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_ours(args):
     import torch
@@ -270,6 +317,11 @@ def run_ours(args):
                "d2h_bytes_per_step": int(opos.nbytes + oalpha.nbytes),
                "wall_s": time.perf_counter() - t0}
 
+    sur = None
+    if rank == 0 and not args.no_surrogate:
+        ctx.close()
+        sur = run_surrogate(args, local)
+
     if rank == 0:
         fp32_peak = capi.fp32_peak(local)
         flops_per_launch = (FLOPS_PER_PAIR * full_timed + FLOPS_PER_FAR_PAIR * (pairs_timed - full_timed)) / max(pair_launches, 1)
@@ -305,9 +357,11 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "surrogate": sur,
         }
         print(json.dumps(out))
-    ctx.close()
+    if sur is None:
+        ctx.close()
     if world > 1:
         dist.destroy_process_group()
 
