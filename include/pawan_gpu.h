@@ -166,7 +166,7 @@ typedef struct pgpu_surrogate_config {
   int leaf_size;       /* particles per octree leaf, 1..512 (default 512) */
   double near_widths;  /* near field: cells closer than this many cube widths (default 4) */
   int order;           /* far-field expansion: 0 monopole, 1 + dipole (default), 2 + quadrupole */
-  int use_mlp;         /* add the learned correction (needs pgpu_surrogate_set_mlp) */
+  int use_mlp;         /* add the learned correction to the order-1 far field (pgpu_surrogate_set_mlp) */
   double tolerance;    /* maximum relative velocity error on the sampled targets (default 1e-4) */
   int check_targets;   /* targets re-checked by the direct sum per evaluation (default 4096, 0 = off) */
   int seed;            /* seed of the sampled targets */
@@ -195,6 +195,40 @@ int pgpu_surrogate_get_stats(pgpu_ctx *ctx, pgpu_surrogate_stats *stats);
  * buffer may be NULL; a buffer smaller than needed is left untouched. */
 int pgpu_surrogate_tree(pgpu_ctx *ctx, int *idx, int64_t idx_cap, int *cell, int64_t cell_cap, int *leaves,
                         int *counts, int64_t leaf_cap, int64_t *n, int64_t *ncells, int64_t *nleaves);
+
+/* ---------------------------------------------------------------------------
+ * Far-field correction network (no PAWAN counterpart).  A 24-128-128-128-6
+ * GELU MLP whose products run on the tensor cores in BF16 with FP32
+ * accumulation (forward, backward and Adam are this library's kernels).  It
+ * predicts, per (target, far cell) pair, the residual of the monopole+dipole
+ * expansion from the cell's moments and the target offset; the features and
+ * output scales are documented in pawan_b200/csrc/treeeval.cuh.  Parameters
+ * are pgpu_mlp_num_params() floats: W1[32][128] (rows 24..31 zero), b1[128],
+ * W2[128][128], b2[128], W3[128][128], b3[128], W4[128][8] (columns 6, 7
+ * zero), b4[8]; a row times W is the layer's pre-activation. */
+typedef struct pgpu_mlp pgpu_mlp;
+int pgpu_mlp_num_params(void);
+int pgpu_mlp_create(pgpu_mlp **mlp, int device, int seed);  /* Glorot-uniform weights from `seed` */
+int pgpu_mlp_destroy(pgpu_mlp *mlp);
+const char *pgpu_mlp_last_error(pgpu_mlp *mlp);
+int pgpu_mlp_get_params(pgpu_mlp *mlp, float *params);
+int pgpu_mlp_set_params(pgpu_mlp *mlp, const float *params);  /* also resets the Adam state */
+/* Outputs (rows x 6) for host feature rows (rows x 24). */
+int pgpu_mlp_forward(pgpu_mlp *mlp, const float *x, int64_t rows, float *y);
+/* Mean-squared-error loss over the rows and its gradient (params layout). */
+int pgpu_mlp_gradient(pgpu_mlp *mlp, const float *x, const float *t, int64_t rows, float *grad, double *loss);
+/* Training set: replace with host rows, or append rows drawn from the octree
+ * of a context's last surrogate evaluation (targets are the exact direct-sum
+ * contribution of the cell minus its monopole+dipole expansion, scaled). */
+int pgpu_mlp_set_dataset(pgpu_mlp *mlp, const float *x, const float *t, int64_t rows);
+int pgpu_mlp_add_samples(pgpu_mlp *mlp, pgpu_ctx *ctx, int64_t nsamples, int seed);
+int64_t pgpu_mlp_dataset_rows(pgpu_mlp *mlp);
+int pgpu_mlp_get_dataset(pgpu_mlp *mlp, float *x, float *t, int64_t max_rows);
+/* Adam (beta 0.9 / 0.999) on random minibatches; loss_history[steps] may be NULL. */
+int pgpu_mlp_train(pgpu_mlp *mlp, int steps, int batch, double lr, int seed, float *loss_history);
+/* Uses a snapshot of the network's current weights for the surrogate's far
+ * field (order-1 expansion + correction) when use_mlp is set. */
+int pgpu_surrogate_set_mlp(pgpu_ctx *ctx, pgpu_mlp *mlp);
 
 /* The context's CUDA stream (a cudaStream_t), so a caller can order its own
  * work or timing events with the library's launches.  No PAWAN counterpart. */

@@ -33,7 +33,10 @@ EXPORTS = [
     "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
     "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
     "pgpu_fp32_peak", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
-    "pgpu_surrogate_disable", "pgpu_surrogate_get_stats", "pgpu_surrogate_tree",
+    "pgpu_surrogate_disable", "pgpu_surrogate_get_stats", "pgpu_surrogate_tree", "pgpu_mlp_num_params",
+    "pgpu_mlp_create", "pgpu_mlp_destroy", "pgpu_mlp_last_error", "pgpu_mlp_get_params", "pgpu_mlp_set_params",
+    "pgpu_mlp_forward", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
+    "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
 ]
 
 
@@ -65,6 +68,7 @@ class PgpuError(RuntimeError):
 
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _i64p = C.POINTER(C.c_int64)
 _lib = None
 
@@ -117,6 +121,20 @@ def load(build_if_missing: bool = False):
         "pgpu_surrogate_enable": (C.c_int, [vp, C.c_int32, C.POINTER(SurrogateConfig)]),
         "pgpu_surrogate_disable": (C.c_int, [vp]),
         "pgpu_surrogate_get_stats": (C.c_int, [vp, C.POINTER(SurrogateStats)]),
+        "pgpu_mlp_num_params": (C.c_int, []),
+        "pgpu_mlp_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int]),
+        "pgpu_mlp_destroy": (C.c_int, [vp]),
+        "pgpu_mlp_last_error": (C.c_char_p, [vp]),
+        "pgpu_mlp_get_params": (C.c_int, [vp, _fp]),
+        "pgpu_mlp_set_params": (C.c_int, [vp, _fp]),
+        "pgpu_mlp_forward": (C.c_int, [vp, _fp, C.c_int64, _fp]),
+        "pgpu_mlp_gradient": (C.c_int, [vp, _fp, _fp, C.c_int64, _fp, _dp]),
+        "pgpu_mlp_set_dataset": (C.c_int, [vp, _fp, _fp, C.c_int64]),
+        "pgpu_mlp_add_samples": (C.c_int, [vp, vp, C.c_int64, C.c_int]),
+        "pgpu_mlp_dataset_rows": (C.c_int64, [vp]),
+        "pgpu_mlp_get_dataset": (C.c_int, [vp, _fp, _fp, C.c_int64]),
+        "pgpu_mlp_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_double, C.c_int, _fp]),
+        "pgpu_surrogate_set_mlp": (C.c_int, [vp, vp]),
         "pgpu_surrogate_tree": (C.c_int, [vp, C.POINTER(C.c_int), C.c_int64, C.POINTER(C.c_int), C.c_int64,
                                           C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int64, _i64p, _i64p, _i64p]),
     }
@@ -305,6 +323,9 @@ class Context:
                                               nl.value, C.byref(n), C.byref(nc), C.byref(nl)))
         return {"idx": idx, "cells": cell, "leaves": leaves, "far": counts[0], "near": counts[1]}
 
+    def surrogate_set_mlp(self, mlp: "Mlp"):
+        self._ck(self.lib.pgpu_surrogate_set_mlp(self.h, mlp.h))
+
     def launch_count(self) -> int:
         return int(self.lib.pgpu_launch_count(self.h))
 
@@ -332,3 +353,85 @@ class Context:
         st = np.zeros(int(6 * m.sum()))
         self._ck(self.lib.pgpu_get_rates_flat(self.h, _p(st), m.ctypes.data_as(_i64p), len(m)))
         return st
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Mlp:
+    """The far-field correction network (see include/pawan_gpu.h)."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.pgpu_mlp_create(C.byref(h), device, seed)
+        if rc != PGPU_OK:
+            raise PgpuError(rc, "pgpu_mlp_create failed")
+        self.h = h
+        self.n_params = int(self.lib.pgpu_mlp_num_params())
+
+    def _ck(self, rc: int):
+        if rc != PGPU_OK:
+            raise PgpuError(rc, self.lib.pgpu_mlp_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pgpu_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        self._ck(self.lib.pgpu_mlp_get_params(self.h, p.ctypes.data_as(_fp)))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = _f32(p)
+        assert p.shape == (self.n_params,)
+        self._ck(self.lib.pgpu_mlp_set_params(self.h, p.ctypes.data_as(_fp)))
+
+    def forward(self, x) -> np.ndarray:
+        x = _f32(x)
+        y = np.zeros((x.shape[0], 6), np.float32)
+        self._ck(self.lib.pgpu_mlp_forward(self.h, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)))
+        return y
+
+    def gradient(self, x, t):
+        x, t = _f32(x), _f32(t)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_double()
+        self._ck(self.lib.pgpu_mlp_gradient(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0],
+                                            g.ctypes.data_as(_fp), C.byref(loss)))
+        return loss.value, g
+
+    def set_dataset(self, x, t):
+        x, t = _f32(x), _f32(t)
+        self._ck(self.lib.pgpu_mlp_set_dataset(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0]))
+
+    def add_samples(self, ctx: Context, n: int, seed: int = 0):
+        self._ck(self.lib.pgpu_mlp_add_samples(self.h, ctx.h, int(n), int(seed)))
+
+    @property
+    def rows(self) -> int:
+        return int(self.lib.pgpu_mlp_dataset_rows(self.h))
+
+    def dataset(self, max_rows: int | None = None):
+        n = self.rows if max_rows is None else min(max_rows, self.rows)
+        x = np.zeros((n, 24), np.float32)
+        t = np.zeros((n, 6), np.float32)
+        self._ck(self.lib.pgpu_mlp_get_dataset(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), n))
+        return x, t
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        hist = np.zeros(max(steps, 1), np.float32)
+        self._ck(self.lib.pgpu_mlp_train(self.h, int(steps), int(batch), float(lr), int(seed),
+                                         hist.ctypes.data_as(_fp)))
+        return hist[:steps]

@@ -835,4 +835,5 @@ const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err.c_str() : "null con
 
 }  // extern "C"
 
+#include "mlp_host.inc"
 #include "surrogate_host.inc"

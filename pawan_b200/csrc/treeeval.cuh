@@ -20,6 +20,7 @@
 // direct kernel.
 #pragma once
 #include "kernels.cuh"
+#include "mlp.cuh"
 #include "tree.cuh"
 
 namespace pgpu {
@@ -120,6 +121,37 @@ __device__ __forceinline__ void far_expand(const float *v, const float *x, const
                       3.f * ir5 * (trP[i] + 2.f * spik);
     s[i] -= 0.5f * d4p;
   }
+}
+
+// Input features of the far-field correction network for one (target, far
+// cell) pair, and the scales of its outputs.  With r = x_t - c, rho = |r|,
+// w the cube width, R the particle spread, A = sum alpha, M the first moment:
+//   0-2 r/rho, 3 4w/rho, 4 4R/rho, 5-7 A/|A|, 8-16 4 M/(|A| rho),
+//   17-19 4 (c - cube centre)/rho, 20-22 alpha_t/|alpha_t|, 23 4 sigma_c/rho
+// The network predicts the residual of the monopole+dipole expansion in units
+// of the quadrupole scale: velocity / (|A| w^2 / rho^4), stretching /
+// (|A| |alpha_t| w^2 / rho^5) (4 pi units).
+__device__ __forceinline__ void far_features(const float *v, const float *x, const float *at, float *f, float &sv,
+                                             float &ss) {
+  const float r[3] = {x[0] - v[0], x[1] - v[1], x[2] - v[2]};
+  const float r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  const float ir = fast_rsqrt(r2);
+  for (int i = 0; i < 3; ++i) f[i] = r[i] * ir;
+  const float w = v[34];
+  f[3] = 4.f * w * ir;
+  f[4] = 4.f * v[33] * ir;
+  const float am = sqrtf(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+  const float ia = am > 0.f ? 1.f / am : 0.f;
+  for (int i = 0; i < 3; ++i) f[5 + i] = v[3 + i] * ia;
+  for (int i = 0; i < 9; ++i) f[8 + i] = 4.f * v[6 + i] * ia * ir;
+  for (int i = 0; i < 3; ++i) f[17 + i] = 4.f * (v[i] - v[35 + i]) * ir;
+  const float tm = sqrtf(at[0] * at[0] + at[1] * at[1] + at[2] * at[2]);
+  const float it = tm > 0.f ? 1.f / tm : 0.f;
+  for (int i = 0; i < 3; ++i) f[20 + i] = at[i] * it;
+  f[23] = 4.f * sqrtf(2.f * v[38]) * ir;
+  const float q2 = (w * ir) * (w * ir);
+  sv = am * ir * ir * q2;
+  ss = am * tm * ir * ir * ir * q2;
 }
 
 // One ordered pair with the FP32 three-regime terms of the direct kernel,
@@ -261,11 +293,24 @@ constexpr int kWarpTile = 64;
 constexpr int kWarpCells = 16;
 constexpr int kWarpsPerCta = 4;
 
+template <bool MLP>
 __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeEvalArgs a, const int2 *items,
-                                                                         int nitems, unsigned *counter) {
+                                                                         int nitems, unsigned *counter,
+                                                                         const MlpPacked *mlp) {
   __shared__ float sc[kWarpsPerCta][kWarpCells][kCellFloats];
   __shared__ float4 sP[kWarpsPerCta][kWarpTile], sQ[kWarpsPerCta][kWarpTile];
+  __shared__ __align__(16) __nv_bfloat16 sF[MLP ? kWarpsPerCta : 1][32][kInPad + 8];
+  __shared__ float sO[MLP ? kWarpsPerCta : 1][32][kOutPad];
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if constexpr (MLP) {
+    // the packed network, shared by the CTA's warps
+    const uint4 *src = reinterpret_cast<const uint4 *>(mlp);
+    uint4 *dst = reinterpret_cast<uint4 *>(dyn_smem);
+    for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
+  const MlpPacked &W = *reinterpret_cast<const MlpPacked *>(dyn_smem);
   for (;;) {
     int item = 0;
     if (lane == 0) item = (int)atomicAdd(counter, 1u);
@@ -292,6 +337,21 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeE
         float u[3], s[3];
         far_expand(sc[w][j], xt, at, a.order, u, s);
         for (int m = 0; m < 3; ++m) { su[m] += u[m]; ss[m] += s[m]; }
+        if constexpr (MLP) {
+          float f[kIn], scv, scs;
+          far_features(sc[w][j], xt, at, f, scv, scs);
+          for (int i = 0; i < kIn; i += 2) *reinterpret_cast<uint32_t *>(&sF[w][lane][i]) = pack_bf16(f[i], f[i + 1]);
+          for (int i = kIn; i < kInPad; i += 2) *reinterpret_cast<uint32_t *>(&sF[w][lane][i]) = 0u;
+          __syncwarp();
+          mlp_tile16(W, sF[w], sO[w], lane);
+          mlp_tile16(W, sF[w] + 16, sO[w] + 16, lane);
+          __syncwarp();
+          for (int m = 0; m < 3; ++m) {
+            su[m] += scv * sO[w][lane][m];
+            ss[m] += scs * sO[w][lane][3 + m];
+          }
+          __syncwarp();
+        }
       }
       for (int m = 0; m < 3; ++m) {
         two_sum_acc(vh[m], vl[m], su[m]);
@@ -323,6 +383,75 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeE
       for (int m = 0; m < 3; ++m) {
         o[m * a.cap] = ((double)vh[m] + (double)vl[m]) * kInv4Pi;
         o[(3 + m) * a.cap] = ((double)dh[m] + (double)dl[m]) * kInv4Pi;
+      }
+    }
+  }
+}
+
+// Training samples of the correction network from the current octree: each
+// warp draws (leaf, target, far cell) with a hash of (seed, sample), computes
+// the features, the exact FP64 contribution of the cell's particles (the
+// direct kernel's formula) and the order-1 expansion, and stores the scaled
+// residual.  Rows whose leaf has no far cell after 32 draws are all zero.
+__global__ void mlp_sample_kernel(TreeEvalArgs a, int nsamples, unsigned long long seed, float *X, float *T) {
+  const int lane = threadIdx.x & 31;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int smp = wg; smp < nsamples; smp += nw) {
+    int li = -1, t = 0, fj = 0;
+    if (lane == 0) {
+      unsigned long long h = seed ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)(smp + 1));
+      for (int tries = 0; tries < 32; ++tries) {
+        h ^= h >> 33; h *= 0xFF51AFD7ED558CCDULL; h ^= h >> 33; h *= 0xC4CEB9FE1A85EC53ULL; h ^= h >> 33;
+        const int l = (int)(h % (unsigned long long)a.nleaves);
+        if (a.far_cnt[l] > 0) {
+          const TreeCell tc = a.cells[a.leaves[l]];
+          li = l;
+          t = tc.start + (int)((h >> 20) % (unsigned long long)(tc.end - tc.start));
+          fj = (int)((h >> 40) % (unsigned long long)a.far_cnt[l]);
+          break;
+        }
+      }
+    }
+    li = __shfl_sync(0xffffffffu, li, 0);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    fj = __shfl_sync(0xffffffffu, fj, 0);
+    float *xo = X + (int64_t)smp * kIn;
+    float *to = T + (int64_t)smp * kOut;
+    if (li < 0) {
+      if (lane < kIn) xo[lane] = 0.f;
+      if (lane < kOut) to[lane] = 0.f;
+      continue;
+    }
+    const int ci = a.far_list[a.far_off[li] + fj];
+    const TreeCell cc = a.cells[ci];
+    const float *v = a.cd[ci].v;
+    const float4 pt = a.Ps[t], qt = a.Qs[t];
+    const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
+    double ex[6] = {0, 0, 0, 0, 0, 0};
+    for (int j = cc.start + lane; j < cc.end; j += 32) {
+      const float4 p = a.Ps[j], q = a.Qs[j];
+      const double d[3] = {(double)pt.x - p.x, (double)pt.y - p.y, (double)pt.z - p.z};
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      const PairTerms<double> k = pair_terms(r2, (double)pt.w + (double)p.w);
+      const double as[3] = {q.x, q.y, q.z}, a_t[3] = {qt.x, qt.y, qt.z};
+      const double w3[3] = {as[1] * d[2] - as[2] * d[1], as[2] * d[0] - as[0] * d[2], as[0] * d[1] - as[1] * d[0]};
+      const double c3[3] = {a_t[1] * as[2] - a_t[2] * as[1], a_t[2] * as[0] - a_t[0] * as[2], a_t[0] * as[1] - a_t[1] * as[0]};
+      const double dc = d[0] * c3[0] + d[1] * c3[1] + d[2] * c3[2];
+      for (int m = 0; m < 3; ++m) {
+        ex[m] += k.q * w3[m];
+        ex[3 + m] += k.q * c3[m] + k.F * dc * d[m];
+      }
+    }
+    for (int m = 0; m < 6; ++m)
+      for (int o = 16; o > 0; o >>= 1) ex[m] += __shfl_down_sync(0xffffffffu, ex[m], o);
+    if (lane == 0) {
+      float f[kIn], scv, scs, u[3], s[3];
+      far_features(v, xt, at, f, scv, scs);
+      far_expand(v, xt, at, 1, u, s);
+      for (int i = 0; i < kIn; ++i) xo[i] = f[i];
+      for (int m = 0; m < 3; ++m) {
+        to[m] = scv > 0.f ? (float)((ex[m] - u[m]) / scv) : 0.f;
+        to[3 + m] = scs > 0.f ? (float)((ex[3 + m] - s[m]) / scs) : 0.f;
       }
     }
   }
