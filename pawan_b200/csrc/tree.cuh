@@ -313,6 +313,10 @@ __global__ void leaf_flags_kernel(const TreeCell *cells, int ncells, int *flag) 
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ncells) flag[i] = cells[i].nchild == 0;
 }
+__global__ void positive_flags_kernel(const int *cnt, int n, int *flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = cnt[i] > 0;
+}
 __global__ void leaf_scatter_kernel(const int *flag, const int *pos, int ncells, int *leaves) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ncells && flag[i]) leaves[pos[i]] = i;

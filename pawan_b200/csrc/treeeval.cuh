@@ -293,16 +293,31 @@ constexpr int kWarpTile = 64;
 constexpr int kWarpCells = 16;
 constexpr int kWarpsPerCta = 4;
 
+// Per-warp shared buffers (all carved from dynamic shared memory, after the
+// packed network when the correction is on).
+struct WarpSmem {
+  float sc[kWarpCells][kCellFloats];
+  float4 sP[kWarpTile], sQ[kWarpTile];
+};
+struct WarpSmemMlp {
+  __nv_bfloat16 sF[32][kInPad + 8];
+  float sO[32][kOutPad];
+};
+constexpr int kWarpsPerCtaMlp = 12;  // warps sharing one copy of the network
+template <bool MLP> constexpr int eval_warps() { return MLP ? kWarpsPerCtaMlp : kWarpsPerCta; }
+template <bool MLP> constexpr size_t eval_smem() {
+  return (MLP ? sizeof(MlpPacked) : 0) + eval_warps<MLP>() * (sizeof(WarpSmem) + (MLP ? sizeof(WarpSmemMlp) : 0));
+}
+
 template <bool MLP>
-__global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeEvalArgs a, const int2 *items,
-                                                                         int nitems, unsigned *counter,
-                                                                         const MlpPacked *mlp) {
-  __shared__ float sc[kWarpsPerCta][kWarpCells][kCellFloats];
-  __shared__ float4 sP[kWarpsPerCta][kWarpTile], sQ[kWarpsPerCta][kWarpTile];
-  __shared__ __align__(16) __nv_bfloat16 sF[MLP ? kWarpsPerCta : 1][32][kInPad + 8];
-  __shared__ float sO[MLP ? kWarpsPerCta : 1][32][kOutPad];
+__global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(TreeEvalArgs a, const int2 *items,
+                                                                             int nitems, unsigned *counter,
+                                                                             const MlpPacked *mlp) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t off0 = MLP ? sizeof(MlpPacked) : 0;
+  WarpSmem &ws = reinterpret_cast<WarpSmem *>(dyn_smem + off0)[w];
+  WarpSmemMlp &wm = reinterpret_cast<WarpSmemMlp *>(dyn_smem + off0 + eval_warps<MLP>() * sizeof(WarpSmem))[w];
   if constexpr (MLP) {
     // the packed network, shared by the CTA's warps
     const uint4 *src = reinterpret_cast<const uint4 *>(mlp);
@@ -330,25 +345,25 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeE
       const int cn = min(kWarpCells, fn - c0);
       __syncwarp();
       for (int e = lane; e < cn * kCellFloats; e += 32)
-        sc[w][e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
+        ws.sc[e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
       __syncwarp();
       float su[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
       for (int j = 0; j < cn; ++j) {
         float u[3], s[3];
-        far_expand(sc[w][j], xt, at, a.order, u, s);
+        far_expand(ws.sc[j], xt, at, a.order, u, s);
         for (int m = 0; m < 3; ++m) { su[m] += u[m]; ss[m] += s[m]; }
         if constexpr (MLP) {
           float f[kIn], scv, scs;
-          far_features(sc[w][j], xt, at, f, scv, scs);
-          for (int i = 0; i < kIn; i += 2) *reinterpret_cast<uint32_t *>(&sF[w][lane][i]) = pack_bf16(f[i], f[i + 1]);
-          for (int i = kIn; i < kInPad; i += 2) *reinterpret_cast<uint32_t *>(&sF[w][lane][i]) = 0u;
+          far_features(ws.sc[j], xt, at, f, scv, scs);
+          for (int i = 0; i < kIn; i += 2) *reinterpret_cast<uint32_t *>(&wm.sF[lane][i]) = pack_bf16(f[i], f[i + 1]);
+          for (int i = kIn; i < kInPad; i += 2) *reinterpret_cast<uint32_t *>(&wm.sF[lane][i]) = 0u;
           __syncwarp();
-          mlp_tile16(W, sF[w], sO[w], lane);
-          mlp_tile16(W, sF[w] + 16, sO[w] + 16, lane);
+          mlp_tile16(W, wm.sF, wm.sO, lane);
+          mlp_tile16(W, wm.sF + 16, wm.sO + 16, lane);
           __syncwarp();
           for (int m = 0; m < 3; ++m) {
-            su[m] += scv * sO[w][lane][m];
-            ss[m] += scs * sO[w][lane][3 + m];
+            su[m] += scv * wm.sO[lane][m];
+            ss[m] += scs * wm.sO[lane][3 + m];
           }
           __syncwarp();
         }
@@ -365,7 +380,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeE
         __syncwarp();
         for (int k = lane; k < kWarpTile; k += 32) {
           const int j = sb + k;
-          if (j < run.y) { sP[w][k] = a.Ps[j]; sQ[w][k] = a.Qs[j]; }
+          if (j < run.y) { ws.sP[k] = a.Ps[j]; ws.sQ[k] = a.Qs[j]; }
         }
         __syncwarp();
         const int cnt = min(kWarpTile, run.y - sb);
@@ -373,7 +388,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeE
           float sv[3] = {}, sd[3] = {}, sp[3] = {}, sdv[3] = {};
           const int gn = min(32, cnt - g);
           for (int jj = 0; jj < gn; ++jj)
-            pair_accum_f32(sP[w][g + jj], sQ[w][g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
+            pair_accum_f32(ws.sP[g + jj], ws.sQ[g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
           fold_group(at, a.nu2, sv, sd, sp, sdv, vh, vl, dh, dl);
         }
       }
@@ -393,24 +408,20 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) tree_eval_warp_kernel(TreeE
 // the features, the exact FP64 contribution of the cell's particles (the
 // direct kernel's formula) and the order-1 expansion, and stores the scaled
 // residual.  Rows whose leaf has no far cell after 32 draws are all zero.
-__global__ void mlp_sample_kernel(TreeEvalArgs a, int nsamples, unsigned long long seed, float *X, float *T) {
+__global__ void mlp_sample_kernel(TreeEvalArgs a, const int *far_leaves, int nfar_leaves, int nsamples,
+                                  unsigned long long seed, float *X, float *T) {
   const int lane = threadIdx.x & 31;
   const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   for (int smp = wg; smp < nsamples; smp += nw) {
     int li = -1, t = 0, fj = 0;
     if (lane == 0) {
       unsigned long long h = seed ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)(smp + 1));
-      for (int tries = 0; tries < 32; ++tries) {
-        h ^= h >> 33; h *= 0xFF51AFD7ED558CCDULL; h ^= h >> 33; h *= 0xC4CEB9FE1A85EC53ULL; h ^= h >> 33;
-        const int l = (int)(h % (unsigned long long)a.nleaves);
-        if (a.far_cnt[l] > 0) {
-          const TreeCell tc = a.cells[a.leaves[l]];
-          li = l;
-          t = tc.start + (int)((h >> 20) % (unsigned long long)(tc.end - tc.start));
-          fj = (int)((h >> 40) % (unsigned long long)a.far_cnt[l]);
-          break;
-        }
-      }
+      h ^= h >> 33; h *= 0xFF51AFD7ED558CCDULL; h ^= h >> 33; h *= 0xC4CEB9FE1A85EC53ULL; h ^= h >> 33;
+      const int l = far_leaves[(int)(h % (unsigned long long)nfar_leaves)];
+      const TreeCell tc = a.cells[a.leaves[l]];
+      li = l;
+      t = tc.start + (int)((h >> 20) % (unsigned long long)(tc.end - tc.start));
+      fj = (int)((h >> 40) % (unsigned long long)a.far_cnt[l]);
     }
     li = __shfl_sync(0xffffffffu, li, 0);
     t = __shfl_sync(0xffffffffu, t, 0);
