@@ -124,31 +124,44 @@ __device__ __forceinline__ void far_expand(const float *v, const float *x, const
 }
 
 // Input features of the far-field correction network for one (target, far
-// cell) pair, and the scales of its outputs.  With r = x_t - c, rho = |r|,
-// w the cube width, R the particle spread, A = sum alpha, M the first moment:
-//   0-2 r/rho, 3 4w/rho, 4 4R/rho, 5-7 A/|A|, 8-16 4 M/(|A| rho),
-//   17-19 4 (c - cube centre)/rho, 20-22 alpha_t/|alpha_t|, 23 4 sigma_c/rho
-// The network predicts the residual of the monopole+dipole expansion in units
-// of the quadrupole scale: velocity / (|A| w^2 / rho^4), stretching /
-// (|A| |alpha_t| w^2 / rho^5) (4 pi units).
+// cell) pair, and the scales of its outputs.  With r = x_t - c (c the cell's
+// particle centroid, the expansion origin), rho = |r|, rh = r/rho, w the cube
+// width, R the particle spread, A = sum alpha, M the first moment and
+// C = sum_a (A_a/|A|) Q_a the strength-weighted second moment about c:
+//   0-2 rh, 3 4w/rho, 4 4R/rho, 5-7 A/|A|, 8-16 4 M/(|A| rho),
+//   17-19 16 C rh/(|A| rho^2), 20-22 alpha_t/|alpha_t|, 23 16 rh.C.rh/(|A| rho^2)
+// For a cell whose strengths share one direction the residual of the
+// monopole+dipole expansion (its quadrupole term) depends on C only through
+// C rh and rh.C.rh, so those projections take the last free slots.  The
+// network predicts that residual in units of the quadrupole scale:
+// velocity / (|A| w^2 / rho^4), stretching / (|A| |alpha_t| w^2 / rho^5)
+// (4 pi units).
 __device__ __forceinline__ void far_features(const float *v, const float *x, const float *at, float *f, float &sv,
                                              float &ss) {
   const float r[3] = {x[0] - v[0], x[1] - v[1], x[2] - v[2]};
   const float r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
   const float ir = fast_rsqrt(r2);
-  for (int i = 0; i < 3; ++i) f[i] = r[i] * ir;
+  const float rh[3] = {r[0] * ir, r[1] * ir, r[2] * ir};
+  for (int i = 0; i < 3; ++i) f[i] = rh[i];
   const float w = v[34];
   f[3] = 4.f * w * ir;
   f[4] = 4.f * v[33] * ir;
   const float am = sqrtf(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
   const float ia = am > 0.f ? 1.f / am : 0.f;
-  for (int i = 0; i < 3; ++i) f[5 + i] = v[3 + i] * ia;
+  const float ah[3] = {v[3] * ia, v[4] * ia, v[5] * ia};
+  for (int i = 0; i < 3; ++i) f[5 + i] = ah[i];
   for (int i = 0; i < 9; ++i) f[8 + i] = 4.f * v[6 + i] * ia * ir;
-  for (int i = 0; i < 3; ++i) f[17 + i] = 4.f * (v[i] - v[35 + i]) * ir;
+  // C = sum_a ah_a Q_a, packed (00,01,02,11,12,22)
+  float Cp[6];
+  for (int e = 0; e < 6; ++e) Cp[e] = ah[0] * v[15 + e] + ah[1] * v[21 + e] + ah[2] * v[27 + e];
+  const float Cr[3] = {Cp[0] * rh[0] + Cp[1] * rh[1] + Cp[2] * rh[2], Cp[1] * rh[0] + Cp[3] * rh[1] + Cp[4] * rh[2],
+                       Cp[2] * rh[0] + Cp[4] * rh[1] + Cp[5] * rh[2]};
+  const float cs = 16.f * ia * ir * ir;
+  for (int i = 0; i < 3; ++i) f[17 + i] = cs * Cr[i];
   const float tm = sqrtf(at[0] * at[0] + at[1] * at[1] + at[2] * at[2]);
   const float it = tm > 0.f ? 1.f / tm : 0.f;
   for (int i = 0; i < 3; ++i) f[20 + i] = at[i] * it;
-  f[23] = 4.f * sqrtf(2.f * v[38]) * ir;
+  f[23] = cs * (rh[0] * Cr[0] + rh[1] * Cr[1] + rh[2] * Cr[2]);
   const float q2 = (w * ir) * (w * ir);
   sv = am * ir * ir * q2;
   ss = am * tm * ir * ir * ir * q2;

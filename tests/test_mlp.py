@@ -90,7 +90,9 @@ def training_set(mlp, n_per_case=200_000):
         c = capi.Context(precision=capi.FP32C, nu=1e-4)
         k = c.add_wake(w.n)
         c.set_particles(k, w)
-        c.surrogate_enable(order=1, check_targets=0)
+        # the 5000-particle ring has far cells only with small leaves; the
+        # features are scale-free, so samples of any leaf size mix
+        c.surrogate_enable(order=1, check_targets=0, leaf_size=32 if w.n < 20_000 else 512)
         c.solve()
         mlp.add_samples(c, n_per_case, seed=i)
         c.close()
