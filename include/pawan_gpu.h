@@ -215,6 +215,9 @@ int pgpu_mlp_get_params(pgpu_mlp *mlp, float *params);
 int pgpu_mlp_set_params(pgpu_mlp *mlp, const float *params);  /* also resets the Adam state */
 /* Outputs (rows x 6) for host feature rows (rows x 24). */
 int pgpu_mlp_forward(pgpu_mlp *mlp, const float *x, int64_t rows, float *y);
+/* The same outputs through the fused warp-level path of the far field
+ * (packed BF16 weights, activations in registers, tanh.approx GELU). */
+int pgpu_mlp_forward_fused(pgpu_mlp *mlp, const float *x, int64_t rows, float *y);
 /* Mean-squared-error loss over the rows and its gradient (params layout). */
 int pgpu_mlp_gradient(pgpu_mlp *mlp, const float *x, const float *t, int64_t rows, float *grad, double *loss);
 /* Training set: replace with host rows, or append rows drawn from the octree

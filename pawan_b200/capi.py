@@ -35,7 +35,7 @@ EXPORTS = [
     "pgpu_fp32_peak", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
     "pgpu_surrogate_disable", "pgpu_surrogate_get_stats", "pgpu_surrogate_tree", "pgpu_mlp_num_params",
     "pgpu_mlp_create", "pgpu_mlp_destroy", "pgpu_mlp_last_error", "pgpu_mlp_get_params", "pgpu_mlp_set_params",
-    "pgpu_mlp_forward", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
+    "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
 ]
 
@@ -128,6 +128,7 @@ def load(build_if_missing: bool = False):
         "pgpu_mlp_get_params": (C.c_int, [vp, _fp]),
         "pgpu_mlp_set_params": (C.c_int, [vp, _fp]),
         "pgpu_mlp_forward": (C.c_int, [vp, _fp, C.c_int64, _fp]),
+        "pgpu_mlp_forward_fused": (C.c_int, [vp, _fp, C.c_int64, _fp]),
         "pgpu_mlp_gradient": (C.c_int, [vp, _fp, _fp, C.c_int64, _fp, _dp]),
         "pgpu_mlp_set_dataset": (C.c_int, [vp, _fp, _fp, C.c_int64]),
         "pgpu_mlp_add_samples": (C.c_int, [vp, vp, C.c_int64, C.c_int]),
@@ -402,6 +403,12 @@ class Mlp:
         x = _f32(x)
         y = np.zeros((x.shape[0], 6), np.float32)
         self._ck(self.lib.pgpu_mlp_forward(self.h, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)))
+        return y
+
+    def forward_fused(self, x) -> np.ndarray:
+        x = _f32(x)
+        y = np.zeros((x.shape[0], 6), np.float32)
+        self._ck(self.lib.pgpu_mlp_forward_fused(self.h, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)))
         return y
 
     def gradient(self, x, t):

@@ -302,6 +302,36 @@ __device__ __forceinline__ void mlp_tile16(const MlpPacked &W, const __nv_bfloat
   O[gid + 8][tig * 2 + 1] = o[3];
 }
 
+// The fused inference path on given rows (one warp per 16-row tile): X[rows][24] -> Y[rows][6].
+__global__ void __launch_bounds__(128) mlp_infer_kernel(const MlpPacked *Wg, const float *X, int rows, float *Y) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  MlpPacked &W = *reinterpret_cast<MlpPacked *>(dyn);
+  __nv_bfloat16 (*F)[kInPad + 8] = reinterpret_cast<__nv_bfloat16 (*)[kInPad + 8]>(dyn + sizeof(MlpPacked));
+  float (*O)[kOutPad] = reinterpret_cast<float (*)[kOutPad]>(dyn + sizeof(MlpPacked) + 4 * 16 * (kInPad + 8) * 2);
+  const uint4 *src = reinterpret_cast<const uint4 *>(Wg);
+  uint4 *dst = reinterpret_cast<uint4 *>(dyn);
+  for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto Fw = F + 16 * w;
+  auto Ow = O + 16 * w;
+  for (int t0 = (blockIdx.x * 4 + w) * 16; t0 < rows; t0 += gridDim.x * 4 * 16) {
+    for (int e = lane; e < 16 * kInPad; e += 32) {
+      const int r = e / kInPad, c = e % kInPad;
+      const int row = t0 + r;
+      Fw[r][c] = __float2bfloat16_rn(c < kIn && row < rows ? X[(int64_t)row * kIn + c] : 0.f);
+    }
+    __syncwarp();
+    mlp_tile16(W, Fw, Ow, lane);
+    __syncwarp();
+    for (int e = lane; e < 16 * kOut; e += 32) {
+      const int r = e / kOut, c = e % kOut;
+      if (t0 + r < rows) Y[(int64_t)(t0 + r) * kOut + c] = Ow[r][c];
+    }
+    __syncwarp();
+  }
+}
+
 // Gathers batch rows of the dataset: X[b][0..31] (features, zero padded), T[b][0..5].
 __global__ void gather_batch_kernel(const float *Xd, const float *Td, const int *rows, int batch, float *X, float *T) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch * kInPad; i += gridDim.x * blockDim.x) {

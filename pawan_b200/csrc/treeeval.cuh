@@ -128,11 +128,13 @@ __device__ __forceinline__ void far_expand(const float *v, const float *x, const
 // particle centroid, the expansion origin), rho = |r|, rh = r/rho, w the cube
 // width, R the particle spread, A = sum alpha, M the first moment and
 // C = sum_a (A_a/|A|) Q_a the strength-weighted second moment about c:
-//   0-2 rh, 3 4w/rho, 4 4R/rho, 5-7 A/|A|, 8-16 4 M/(|A| rho),
+//   0-2 rh, 3 4w/rho, 4 4 sigma_c/rho, 5-7 A/|A|, 8-16 4 M/(|A| rho),
 //   17-19 16 C rh/(|A| rho^2), 20-22 alpha_t/|alpha_t|, 23 16 rh.C.rh/(|A| rho^2)
 // For a cell whose strengths share one direction the residual of the
 // monopole+dipole expansion (its quadrupole term) depends on C only through
-// C rh and rh.C.rh, so those projections take the last free slots.  The
+// C rh and rh.C.rh, so those projections take the last free slots; sigma_c
+// (the cell's mean smoothing radius) carries what is left of the Gaussian
+// regularisation for cells only a few radii away.  The
 // network predicts that residual in units of the quadrupole scale:
 // velocity / (|A| w^2 / rho^4), stretching / (|A| |alpha_t| w^2 / rho^5)
 // (4 pi units).
@@ -145,7 +147,7 @@ __device__ __forceinline__ void far_features(const float *v, const float *x, con
   for (int i = 0; i < 3; ++i) f[i] = rh[i];
   const float w = v[34];
   f[3] = 4.f * w * ir;
-  f[4] = 4.f * v[33] * ir;
+  f[4] = 4.f * sqrtf(2.f * v[38]) * ir;
   const float am = sqrtf(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
   const float ia = am > 0.f ? 1.f / am : 0.f;
   const float ah[3] = {v[3] * ia, v[4] * ia, v[5] * ia};

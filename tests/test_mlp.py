@@ -39,6 +39,16 @@ def test_forward_matches_oracle(gpu):
 
 
 @pytest.mark.gpu
+def test_fused_inference_matches_forward(gpu):
+    """The warp-level path the far field uses gives the training network's outputs."""
+    m = capi.Mlp(seed=9)
+    x = np.random.default_rng(6).normal(size=(1001, R.IN)).astype(np.float32)
+    y = m.forward(x)
+    yf = m.forward_fused(x)
+    assert np.abs(yf - y).max() <= 1e-2 * np.abs(y).max()
+
+
+@pytest.mark.gpu
 def test_gradient_matches_oracle(gpu):
     """BF16 operands with FP32 accumulation against FP64: per-tensor relative
     error of the gradient below 5e-2."""
