@@ -242,6 +242,31 @@ int pgpu_get_stream(pgpu_ctx *ctx, void **stream);
  * roofline denominators.  No PAWAN counterpart. */
 int pgpu_fp32_peak(int device, double *tflops, double *ms);
 
+/* Largest system pgpu_rates_noalloc accepts (its fixed scratch: ~13.6 MB of
+ * device memory per GPU, held from library load until process exit). */
+#define PGPU_NOALLOC_MAX_N 32768
+
+/* Velocity and dalpha/dt of one system of n <= PGPU_NOALLOC_MAX_N particles,
+ * FP32C pair terms as pgpu_solve computes them (no freestream added), for
+ * callers that must not allocate device memory: a host whose own pool owns
+ * all of the GPU's memory, or a real-time loop where cudaMalloc would
+ * synchronise the device.  No counterpart in PAWAN, which has no device code.
+ *
+ * All arrays are DEVICE pointers, row-major FP64: pos, alpha, vel, dalpha
+ * (n, 3); sigma, vol (n).  Work is queued on `stream` (a cudaStream_t, NULL
+ * for the legacy default stream); the call does not wait for it.  It never
+ * calls cudaMalloc or cudaFree: its intermediates live in one static device
+ * array.  The first call on each device looks up that array's address and
+ * clears its work counters (a blocking memset), so make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU (different
+ * streams, or host threads without ordering) race and must not be issued.
+ * n > PGPU_NOALLOC_MAX_N is rejected with PGPU_EINVAL; the reason is in
+ * pgpu_noalloc_last_error(). */
+int pgpu_rates_noalloc(const double *pos, const double *alpha, const double *sigma, const double *vol, int64_t n,
+                       double nu, double *vel, double *dalpha, void *stream);
+/* Message for the last pgpu_rates_noalloc failure on the calling thread ("" after a success). */
+const char *pgpu_noalloc_last_error(void);
+
 const char *pgpu_last_error(pgpu_ctx *ctx);
 const char *pgpu_version(void);
 

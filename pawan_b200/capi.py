@@ -37,6 +37,7 @@ EXPORTS = [
     "pgpu_mlp_create", "pgpu_mlp_destroy", "pgpu_mlp_last_error", "pgpu_mlp_get_params", "pgpu_mlp_set_params",
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
+    "pgpu_rates_noalloc", "pgpu_noalloc_last_error",
 ]
 
 
@@ -138,6 +139,8 @@ def load(build_if_missing: bool = False):
         "pgpu_surrogate_set_mlp": (C.c_int, [vp, vp]),
         "pgpu_surrogate_tree": (C.c_int, [vp, C.POINTER(C.c_int), C.c_int64, C.POINTER(C.c_int), C.c_int64,
                                           C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int64, _i64p, _i64p, _i64p]),
+        "pgpu_rates_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int64, C.c_double, vp, vp, vp]),
+        "pgpu_noalloc_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -163,6 +166,19 @@ def fp32_peak(device: int = 0) -> float:
     if rc != PGPU_OK:
         raise PgpuError(rc, "pgpu_fp32_peak failed")
     return tf.value
+
+
+NOALLOC_MAX_N = 32768  # PGPU_NOALLOC_MAX_N
+
+
+def rates_noalloc(pos: int, alpha: int, sigma: int, vol: int, n: int, nu: float, vel: int, dalpha: int,
+                  stream: int = 0) -> None:
+    """pgpu_rates_noalloc on device addresses (row-major FP64 (n, 3) / (n,)
+    arrays); queues the work on `stream` and returns without waiting."""
+    lib = load()
+    rc = lib.pgpu_rates_noalloc(pos, alpha, sigma, vol, n, nu, vel, dalpha, stream or None)
+    if rc != PGPU_OK:
+        raise PgpuError(rc, lib.pgpu_noalloc_last_error().decode())
 
 
 def kernel_shapes() -> list[tuple[int, int]]:

@@ -381,7 +381,7 @@ __global__ void pack_kernel(const double *x0, const double *sig, const double *v
 
 // Host row-major (n, 3) position / strength + (n) radius / volume, staged in
 // device memory, scattered into the SoA state at slot offset `off`.
-__global__ void scatter_kernel(const double *stage, int64_t n, int64_t off, int64_t cap, double *x0, double *sig,
+static __global__ void scatter_kernel(const double *stage, int64_t n, int64_t off, int64_t cap, double *x0, double *sig,
                                double *vol) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
@@ -395,7 +395,7 @@ __global__ void scatter_kernel(const double *stage, int64_t n, int64_t off, int6
 }
 
 // SoA [6][cap] (from slot offset `off`) -> row-major (n, 3) x 2.
-__global__ void gather_kernel(const double *src, int64_t n, int64_t off, int64_t cap, double *stage) {
+static __global__ void gather_kernel(const double *src, int64_t n, int64_t off, int64_t cap, double *stage) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
@@ -408,7 +408,7 @@ __global__ void gather_kernel(const double *src, int64_t n, int64_t off, int64_t
 // Flat PAWAN state vector (per wake [x (maxN x 3) ; alpha (maxN x 3)] at offset
 // sum of 6 maxN, __interaction::setStates/getStates, interaction.cpp:337-365,
 // wake.cpp:856-893) <-> SoA state.  dir = 0: flat -> SoA, 1: SoA -> flat.
-__global__ void flat_kernel(double *flat, int64_t n, int64_t maxn, int64_t off, int64_t cap, double *soa, int dir) {
+static __global__ void flat_kernel(double *flat, int64_t n, int64_t maxn, int64_t off, int64_t cap, double *soa, int dir) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
@@ -518,7 +518,7 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
   return r;
 }
 
-__global__ void diag_wake_kernel(const double *x0, const double *sig, const double *partial, int nch, int64_t cap,
+static __global__ void diag_wake_kernel(const double *x0, const double *sig, const double *partial, int nch, int64_t cap,
                                  int64_t lo, int64_t hi, int quad, double *out) {
   __shared__ double red[32];
   double f[kDiagFields];
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(BLOCK) probe_kernel(const double *x0, const do
 // all operands in registers.  The result is stored only if it equals a value
 // it cannot take, so the loop is not eliminated.
 constexpr int kFfmaChains = 8;
-__global__ void __launch_bounds__(256) ffma_peak_kernel(float *out, int iters, float a, float b) {
+static __global__ void __launch_bounds__(256) ffma_peak_kernel(float *out, int iters, float a, float b) {
   float x[kFfmaChains];
 #pragma unroll
   for (int k = 0; k < kFfmaChains; ++k) x[k] = threadIdx.x * 1e-3f + k;
