@@ -126,18 +126,22 @@ __device__ __forceinline__ void far_expand(const float *v, const float *x, const
 // Input features of the far-field correction network for one (target, far
 // cell) pair, and the scales of its outputs.  With r = x_t - c (c the cell's
 // particle centroid, the expansion origin), rho = |r|, rh = r/rho, w the cube
-// width, R the particle spread, A = sum alpha, M the first moment and
-// C = sum_a (A_a/|A|) Q_a the strength-weighted second moment about c:
-//   0-2 rh, 3 4w/rho, 4 4 sigma_c/rho, 5-7 A/|A|, 8-16 4 M/(|A| rho),
-//   17-19 16 C rh/(|A| rho^2), 20-22 alpha_t/|alpha_t|, 23 16 rh.C.rh/(|A| rho^2)
-// For a cell whose strengths share one direction the residual of the
-// monopole+dipole expansion (its quadrupole term) depends on C only through
-// C rh and rh.C.rh, so those projections take the last free slots; sigma_c
-// (the cell's mean smoothing radius) carries what is left of the Gaussian
-// regularisation for cells only a few radii away.  The
-// network predicts that residual in units of the quadrupole scale:
-// velocity / (|A| w^2 / rho^4), stretching / (|A| |alpha_t| w^2 / rho^5)
-// (4 pi units).
+// width, A = sum alpha, Q_j = sum alpha_j y y^T (y = x_s - c) the second
+// moments and C = sum_j (A_j/|A|) Q_j:
+//   0-2 rh, 3 4w/rho, 4 4 sigma_c/rho, 5-7 A/|A|,
+//   8-10 4 eps_ijk (Q_j rh)_k / (|A| w^2), 11-13 4 rh.Q_j.rh / (|A| w^2),
+//   14-16 4 tr Q_j / (|A| w^2), 17-19 16 C rh/(|A| rho^2),
+//   20-22 alpha_t/|alpha_t|, 23 16 rh.C.rh/(|A| rho^2)
+// The residual of the monopole+dipole expansion is led by the quadrupole
+// term, whose velocity is exactly
+//   (-3 eps_ijk (Q_j rh)_k + (7.5 rh.Q_j.rh - 1.5 tr Q_j) (e_j x rh)_i) / rho^4
+// (4 pi units), a function of slots 0-2 and 8-16 alone; its stretching
+// also involves alpha_t, and for strengths close to one direction (Q_j ~
+// A_j C / |A|) it depends on C through C rh and rh.C.rh.  sigma_c (the cell's
+// mean smoothing radius) carries what is left of the Gaussian regularisation
+// for cells only a few radii away.  The network predicts the residual in
+// units of the quadrupole scale: velocity / (|A| w^2 / rho^4), stretching /
+// (|A| |alpha_t| w^2 / rho^5) (4 pi units).
 __device__ __forceinline__ void far_features(const float *v, const float *x, const float *at, float *f, float &sv,
                                              float &ss) {
   const float r[3] = {x[0] - v[0], x[1] - v[1], x[2] - v[2]};
@@ -152,7 +156,19 @@ __device__ __forceinline__ void far_features(const float *v, const float *x, con
   const float ia = am > 0.f ? 1.f / am : 0.f;
   const float ah[3] = {v[3] * ia, v[4] * ia, v[5] * ia};
   for (int i = 0; i < 3; ++i) f[5 + i] = ah[i];
-  for (int i = 0; i < 9; ++i) f[8 + i] = 4.f * v[6 + i] * ia * ir;
+  const float qs = w > 0.f ? 4.f * ia / (w * w) : 0.f;
+  float P[3][3];  // P[j] = Q_j rh
+  for (int j = 0; j < 3; ++j) {
+    const float *Q = v + 15 + 6 * j;
+    P[j][0] = Q[0] * rh[0] + Q[1] * rh[1] + Q[2] * rh[2];
+    P[j][1] = Q[1] * rh[0] + Q[3] * rh[1] + Q[4] * rh[2];
+    P[j][2] = Q[2] * rh[0] + Q[4] * rh[1] + Q[5] * rh[2];
+    f[11 + j] = qs * (rh[0] * P[j][0] + rh[1] * P[j][1] + rh[2] * P[j][2]);
+    f[14 + j] = qs * (Q[0] + Q[3] + Q[5]);
+  }
+  f[8] = qs * (P[1][2] - P[2][1]);
+  f[9] = qs * (P[2][0] - P[0][2]);
+  f[10] = qs * (P[0][1] - P[1][0]);
   // C = sum_a ah_a Q_a, packed (00,01,02,11,12,22)
   float Cp[6];
   for (int e = 0; e < 6; ++e) Cp[e] = ah[0] * v[15 + e] + ah[1] * v[21 + e] + ah[2] * v[27 + e];
