@@ -119,12 +119,59 @@ __device__ __forceinline__ bool next_item(unsigned int *counters, int64_t total,
 }
 
 // ---------------------------------------------------------------- pair kernel
+// Axis-aligned box of points held by the lanes of a warp, with the largest
+// sigma^2/2 among them; after reduce() every lane holds the warp's box.
+struct WarpBox {
+  float lo[3], hi[3], hs;
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int m = 0; m < 3; ++m) { lo[m] = 3.0e38f; hi[m] = -3.0e38f; }
+    hs = 0.f;
+  }
+  __device__ __forceinline__ void add(float x, float y, float z, float h) {
+    lo[0] = fminf(lo[0], x); hi[0] = fmaxf(hi[0], x);
+    lo[1] = fminf(lo[1], y); hi[1] = fmaxf(hi[1], y);
+    lo[2] = fminf(lo[2], z); hi[2] = fmaxf(hi[2], z);
+    hs = fmaxf(hs, h);
+  }
+  __device__ __forceinline__ void reduce() {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        lo[m] = fminf(lo[m], __shfl_xor_sync(0xffffffffu, lo[m], o));
+        hi[m] = fmaxf(hi[m], __shfl_xor_sync(0xffffffffu, hi[m], o));
+      }
+      hs = fmaxf(hs, __shfl_xor_sync(0xffffffffu, hs, o));
+    }
+  }
+};
+
+// True when every (target, source) pair of the two boxes has u = r^2 /
+// (hs_t + hs_s) >= kFarU: the squared gap between the boxes is a lower bound
+// of every pair's r^2.  A zero gap (touching or overlapping boxes, coincident
+// particles) is never far.
+__device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s) {
+  float d2 = 0.f;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const float gap = fmaxf(fmaxf(s.lo[m] - t.hi[m], t.lo[m] - s.hi[m]), 0.f);
+    d2 = fmaf(gap, gap, d2);
+  }
+  return d2 > 0.f && d2 >= kFarU * (t.hs + s.hs);
+}
+
 // BLOCK threads, TPT targets per thread, TILE sources per shared-memory tile
 // (TILE == BLOCK: each thread stages one record), CG sources per compensation
 // group (plain FP32 partial sums over CG sources, then an error-free two-sum
 // into the per-target (hi, lo) accumulators).
+// FP32: at most 64 registers per target held, so that 2048 targets are
+// resident per SM (e.g. 4 CTAs of 256 threads with one target each).
+template <typename T, int BLOCK, int TPT>
+constexpr int pair_min_blocks() { return sizeof(T) == 4 ? 65536 / (BLOCK * 64 * TPT) : 1; }
+
 template <typename T, int BLOCK, int TPT, int CG>
-__global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
+__global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pair_kernel(PairArgs<T> a) {
   constexpr int TILE = BLOCK;
   constexpr int TT = BLOCK * TPT;
   static_assert(TILE % CG == 0, "compensation group must divide the tile");
@@ -132,6 +179,7 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
   __shared__ __align__(16) v4_t<T> sQ[2][TILE];
   __shared__ int s_item;
   const int tid = threadIdx.x;
+  const int lane = tid & 31;
   const int64_t total = a.plan[a.nsys].item_start;
   int64_t item;
   while (next_item(a.counters, total, item, &s_item)) {
@@ -160,6 +208,15 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
 #pragma unroll
       for (int m = 0; m < 3; ++m) { vh[k][m] = 0; vl[k][m] = 0; dh[k][m] = 0; dl[k][m] = 0; }
     }
+    // FP32: bounding box of this warp's targets and their largest sigma^2/2,
+    // for the per-tile all-far test below
+    WarpBox tb;
+    if constexpr (sizeof(T) == 4) {
+      tb.init();
+#pragma unroll
+      for (int k = 0; k < TPT; ++k) tb.add(xt[k][0], xt[k][1], xt[k][2], hst[k]);
+      tb.reduce();
+    }
 
     // Stage the first tile.
     int buf = 0;
@@ -181,6 +238,24 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
       cp_async_wait<1>();
       __syncthreads();
 
+      // FP32: every pair of this warp's targets with this tile's sources is
+      // far (u >= 50) when the boxes are at least sqrt(50 (hs_t + hs_s)) apart
+      // in every case; such tiles take the far limit with no per-pair test.
+      // The boxes' distance is a lower bound of every pair's, so a far pair
+      // is never misclassified near; a pair within rounding of u = 50 may take
+      // the far limit, whose dropped terms are below 2e-9 there.
+      bool far_tile = false;
+      if constexpr (sizeof(T) == 4) {
+        WarpBox sb_box;
+        sb_box.init();
+        for (int r = lane; r < TILE; r += 32) {
+          const v4_t<T> p = sP[buf][r];
+          sb_box.add(p.x, p.y, p.z, p.w);
+        }
+        sb_box.reduce();
+        far_tile = all_far(tb, sb_box);
+      }
+
 #pragma unroll 1
       for (int g = 0; g < TILE; g += CG) {
         T sv[TPT][3], sd[TPT][3], sp[TPT][3], sdv[TPT][3];
@@ -189,6 +264,30 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
 #pragma unroll
           for (int m = 0; m < 3; ++m) { sv[k][m] = 0; sd[k][m] = 0; sp[k][m] = 0; sdv[k][m] = 0; }
         }
+        if (far_tile) {
+#pragma unroll 4
+          for (int jj = 0; jj < CG; ++jj) {
+            const v4_t<T> p = sP[buf][g + jj];
+            const v4_t<T> q = sQ[buf][g + jj];
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) {
+              const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
+              const T r2 = dx * dx + dy * dy + dz * dz;
+              // far limit: q' = r^3, F' = -3 r^5, no diffusion
+              const float ir = fast_rsqrt(r2);
+              const float A = ir * ir;
+              const T qq = A * ir;
+              const T FF = -3.0f * qq * A;
+              const T wx = q.y * dz - q.z * dy;
+              const T wy = q.z * dx - q.x * dz;
+              const T wz = q.x * dy - q.y * dx;
+              sv[k][0] += qq * wx; sv[k][1] += qq * wy; sv[k][2] += qq * wz;
+              const T fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
+              sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
+              sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
+            }
+          }
+        } else {
 #pragma unroll 4
         for (int jj = 0; jj < CG; ++jj) {
           const v4_t<T> p = sP[buf][g + jj];
@@ -198,8 +297,6 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
             const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
             const T r2 = dx * dx + dy * dy + dz * dz;
             T qq, FF;
-            bool diffuse;
-            T zd = 0;
             if constexpr (sizeof(T) == 4) {
               // far test r^2 >= 50 (hs_t + hs_s) as one FMA against the
               // target's precomputed 50 hs_t
@@ -209,21 +306,26 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
               const float A = ir * ir;
               qq = A * ir;
               FF = -3.0f * qq * A;
-              diffuse = false;
               // the full formula only when some lane of the warp needs it:
               // the vote keeps the common all-far case free of divergence
               if (__any_sync(0xffffffffu, near)) {
                 if (near) {
                   const PairTerms<float> pt = pair_terms_near(r2, hst[k] + p.w);
-                  qq = pt.q; FF = pt.F; zd = pt.zd;
-                  diffuse = true;
+                  qq = pt.q; FF = pt.F;
+                  // v_t a_s - v_s a_t per pair, so nearly equal strengths cancel
+                  // before they are summed (as in DIFFUSION, interaction_utils.h:358-369)
+                  sdv[k][0] += pt.zd * (vt[k] * q.x - q.w * at[k][0]);
+                  sdv[k][1] += pt.zd * (vt[k] * q.y - q.w * at[k][1]);
+                  sdv[k][2] += pt.zd * (vt[k] * q.z - q.w * at[k][2]);
                   ++nfull;
                 }
               }
             } else {
               const PairTerms<T> pt = pair_terms(r2, hst[k] + p.w);
-              qq = pt.q; FF = pt.F; zd = pt.zd;
-              diffuse = true;
+              qq = pt.q; FF = pt.F;
+              sdv[k][0] += pt.zd * (vt[k] * q.x - q.w * at[k][0]);
+              sdv[k][1] += pt.zd * (vt[k] * q.y - q.w * at[k][1]);
+              sdv[k][2] += pt.zd * (vt[k] * q.z - q.w * at[k][2]);
             }
             // w = alpha_s x d
             const T wx = q.y * dz - q.z * dy;
@@ -234,14 +336,8 @@ __global__ void __launch_bounds__(BLOCK) pair_kernel(PairArgs<T> a) {
             const T fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
             sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
             sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
-            if (diffuse) {
-              // v_t a_s - v_s a_t per pair, so nearly equal strengths cancel
-              // before they are summed (as in DIFFUSION, interaction_utils.h:358-369)
-              sdv[k][0] += zd * (vt[k] * q.x - q.w * at[k][0]);
-              sdv[k][1] += zd * (vt[k] * q.y - q.w * at[k][1]);
-              sdv[k][2] += zd * (vt[k] * q.z - q.w * at[k][2]);
-            }
           }
+        }
         }
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
