@@ -30,6 +30,9 @@
 namespace pgpu {
 
 constexpr int kMaxChunks = 16;
+// Sources per compensation group of the FP32 pair kernel: plain FP32 partial
+// sums over this many sources, then one error-free two-sum per component.
+constexpr int kPairCG = 64;
 constexpr int kDiagFields = 19;
 
 // One system in the work list (sorted by decreasing work).
@@ -208,6 +211,13 @@ __global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pai
 #pragma unroll
       for (int m = 0; m < 3; ++m) { vh[k][m] = 0; vl[k][m] = 0; dh[k][m] = 0; dl[k][m] = 0; }
     }
+    // -3 alpha_t: the far limit's F' = -3 r^5 with the constant folded in
+    T at3[TPT][3];
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+      for (int m = 0; m < 3; ++m) at3[k][m] = T(-3) * at[k][m];
+    }
     // FP32: bounding box of this warp's targets and their largest sigma^2/2,
     // for the per-tile all-far test below
     WarpBox tb;
@@ -273,16 +283,15 @@ __global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pai
             for (int k = 0; k < TPT; ++k) {
               const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
               const T r2 = dx * dx + dy * dy + dz * dz;
-              // far limit: q' = r^3, F' = -3 r^5, no diffusion
+              // far limit: q' = r^3, F' = -3 r^5 (the -3 is in at3), no diffusion
               const float ir = fast_rsqrt(r2);
               const float A = ir * ir;
               const T qq = A * ir;
-              const T FF = -3.0f * qq * A;
               const T wx = q.y * dz - q.z * dy;
               const T wy = q.z * dx - q.x * dz;
               const T wz = q.x * dy - q.y * dx;
               sv[k][0] += qq * wx; sv[k][1] += qq * wy; sv[k][2] += qq * wz;
-              const T fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
+              const T fd = (qq * A) * (at3[k][0] * wx + at3[k][1] * wy + at3[k][2] * wz);
               sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
               sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
             }

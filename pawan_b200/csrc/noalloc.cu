@@ -39,7 +39,7 @@ namespace {
 constexpr int64_t kNoAllocMaxN = PGPU_NOALLOC_MAX_N;
 constexpr int kNoAllocChunks = 8;
 constexpr int kNoAllocBlock = 256;  // one target per thread, 256-source tiles
-constexpr int kNoAllocCG = 32;      // sources per compensation group, as in the context path
+constexpr int kNoAllocCG = kPairCG;  // sources per compensation group, as in the context path
 
 // Carve-up of the scratch array (byte offsets, each 256-aligned).
 constexpr size_t kOffP = 0;

@@ -31,7 +31,7 @@ using namespace pgpu;
 
 namespace {
 
-constexpr int kCG = 32;
+constexpr int kCG = kPairCG;
 
 struct Shape { int block, tpt; };
 // Compiled pair-kernel shapes (the autotuner chooses among these).

@@ -1,6 +1,6 @@
 """A small, self-contained workload for profilers (ncu) and quick timing.
 
-    python -m pawan_b200.profile_case [--stations 200] [--solves 3] [--fp64] [--steps 1]
+    python -m pawan_b200.profile_case [--stations 200] [--solves 3] [--fp64] [--steps 1] [--block 256 --tpt 2]
 
 Builds the Gaussian-core vortex ring of the 1M-particle benchmark with
 ``stations`` x 1000 particles (200 -> N = 200,000), runs ``solves`` rate
@@ -21,9 +21,11 @@ def main() -> None:
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--block", type=int, default=0, help="pair-kernel block size (0: library default)")
+    ap.add_argument("--tpt", type=int, default=0, help="targets per thread (0: library default)")
     a = ap.parse_args()
     w = cases.ring_gaussian(stations=a.stations, per_section=1000, sigma=0.02, seed=1)
-    c = capi.Context(precision=capi.FP64 if a.fp64 else capi.FP32C, nu=1e-4)
+    c = capi.Context(precision=capi.FP64 if a.fp64 else capi.FP32C, nu=1e-4, block=a.block, tpt=a.tpt)
     k = c.add_wake(w.n)
     c.set_particles(k, w)
     for _ in range(a.solves):
