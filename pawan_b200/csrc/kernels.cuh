@@ -168,13 +168,10 @@ __device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s) {
 // (TILE == BLOCK: each thread stages one record), CG sources per compensation
 // group (plain FP32 partial sums over CG sources, then an error-free two-sum
 // into the per-target (hi, lo) accumulators).
-// FP32: at most 64 registers per target held, so that 2048 targets are
-// resident per SM (e.g. 4 CTAs of 256 threads with one target each).
-template <typename T, int BLOCK, int TPT>
-constexpr int pair_min_blocks() { return sizeof(T) == 4 ? 65536 / (BLOCK * 64 * TPT) : 1; }
-
+// This generic body serves the FP64 mode; the FP32 mode uses
+// pair_body_f32 (pair_f32.cuh), the same decomposition with packed FP32.
 template <typename T, int BLOCK, int TPT, int CG>
-__global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pair_kernel(PairArgs<T> a) {
+__device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
   constexpr int TILE = BLOCK;
   constexpr int TT = BLOCK * TPT;
   static_assert(TILE % CG == 0, "compensation group must divide the tile");
@@ -385,6 +382,21 @@ __global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pai
       }
     }
   }
+}
+
+}  // namespace pgpu
+
+#include "pair_f32.cuh"
+
+namespace pgpu {
+
+template <typename T, int BLOCK, int TPT>
+constexpr int pair_min_blocks() { return sizeof(T) == 4 ? pair_f32_min_blocks<BLOCK, TPT>() : 1; }
+
+template <typename T, int BLOCK, int TPT, int CG>
+__global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pair_kernel(PairArgs<T> a) {
+  if constexpr (sizeof(T) == 4) pair_body_f32<BLOCK, TPT, CG>(a);
+  else pair_body_generic<T, BLOCK, TPT, CG>(a);
 }
 
 // ---------------------------------------------------------------- stage kernel

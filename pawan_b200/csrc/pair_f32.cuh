@@ -1,0 +1,278 @@
+// FP32 (compensated) body of the direct pair kernel.
+//
+// Same work decomposition as the generic body in kernels.cuh: persistent
+// CTAs take (system, target tile, source chunk) items; each thread holds TPT
+// targets; source tiles of TILE = BLOCK records are double-buffered in shared
+// memory with cp.async.  What differs is the arithmetic layout:
+//
+// * Sources are processed in pairs with the packed two-wide FP32 instructions
+//   of sm_100 (__ffma2_rn / __fmul2_rn): lane .x of every float2 belongs to
+//   the even source of a pair, lane .y to the odd one.  One packed
+//   instruction does two pairs' work in one issue slot, which leaves issue
+//   slots for the loads, the rsqrt and the loop, so the FP32 pipe, not the
+//   issue rate, bounds the kernel.  The per-lane results are the IEEE
+//   round-to-nearest results of the scalar operations.
+// * The tile is staged pair-interleaved: for source pair r, float4 2r holds
+//   (x0, x1, y0, y1) and 2r+1 holds (z0, z1, hs0, hs1); Q likewise with
+//   (ax0, ax1, ay0, ay1), (az0, az1, vol0, vol1).  Each source is copied with
+//   four 4-byte cp.async per record, so one 16-byte shared load yields two
+//   float2 operands.
+// * Cross products stay scalar, where a negated operand is free.
+#pragma once
+
+namespace pgpu {
+
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+
+// FP32: about 48 + 32 TPT registers per thread; enough CTAs per SM to hold
+// them (e.g. 3 CTAs of 256 threads with one target each).
+template <int BLOCK, int TPT>
+constexpr int pair_f32_min_blocks() {
+  return 65536 / (BLOCK * (48 + 32 * TPT)) > 0 ? 65536 / (BLOCK * (48 + 32 * TPT)) : 1;
+}
+
+template <int BLOCK, int TPT, int CG>
+__device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
+  constexpr int TILE = BLOCK;
+  constexpr int TT = BLOCK * TPT;
+  constexpr int NPR = TILE / 2;  // source pairs per tile
+  static_assert(TILE % CG == 0 && CG % 2 == 0, "compensation group must divide the tile into source pairs");
+  __shared__ __align__(16) float4 sP[2][TILE];
+  __shared__ __align__(16) float4 sQ[2][TILE];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const float2 M1 = make_float2(-1.f, -1.f);
+  const int64_t total = a.plan[a.nsys].item_start;
+  int64_t item;
+  while (next_item(a.counters, total, item, &s_item)) {
+    const int si = find_plan(a.plan, a.nsys, item);
+    const PlanEntry pe = a.plan[si];
+    const int64_t local = item - pe.item_start;
+    const int64_t tile = local / a.nch;
+    const int c = (int)(local - tile * a.nch);
+    const int64_t t0 = pe.off + tile * TT;
+    const int64_t tend = pe.off + pe.n;
+    const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
+    const int64_t s1 = min(s0 + pe.chunk, tend);
+
+    // targets: scalar copies for the near path and the fold, duplicated
+    // float2 copies for the packed far loop
+    float xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT], h50[TPT];
+    float2 X[TPT][3], AT3[TPT][3];
+    float vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
+    unsigned nfull = 0;  // pairs evaluated with the full (non-far) formula, self pairs included
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      int64_t ti = t0 + tid + k * BLOCK;
+      ti = ti < tend ? ti : tend - 1;
+      const float4 p = a.P[ti];
+      const float4 q = a.Q[ti];
+      xt[k][0] = p.x; xt[k][1] = p.y; xt[k][2] = p.z; hst[k] = p.w;
+      h50[k] = kFarU * p.w;
+      at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        X[k][m] = make_float2(xt[k][m], xt[k][m]);
+        // -3 alpha_t: the far limit's F' = -3 r^5 with the constant folded in
+        AT3[k][m] = make_float2(-3.f * at[k][m], -3.f * at[k][m]);
+        vh[k][m] = 0.f; vl[k][m] = 0.f; dh[k][m] = 0.f; dl[k][m] = 0.f;
+      }
+    }
+    // bounding box of this warp's targets and their largest sigma^2/2, for
+    // the per-tile all-far test
+    WarpBox tb;
+    tb.init();
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) tb.add(xt[k][0], xt[k][1], xt[k][2], hst[k]);
+    tb.reduce();
+
+    // Stage source j into buffer b at its pair-interleaved place.
+    auto stage = [&](int b, int64_t j) {
+      float *dp = reinterpret_cast<float *>(&sP[b][0]) + (tid >> 1) * 8 + (tid & 1);
+      float *dq = reinterpret_cast<float *>(&sQ[b][0]) + (tid >> 1) * 8 + (tid & 1);
+      if (j < s1) {
+        const float *gp = reinterpret_cast<const float *>(a.P + j);
+        const float *gq = reinterpret_cast<const float *>(a.Q + j);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { cp_async4(dp + 2 * m, gp + m); cp_async4(dq + 2 * m, gq + m); }
+      } else {
+        // padding source: far away, zero strength and volume (pad_P / pad_Q)
+        dp[0] = 1e18f; dp[2] = 1e18f; dp[4] = 1e18f; dp[6] = 1.f;
+        dq[0] = 0.f; dq[2] = 0.f; dq[4] = 0.f; dq[6] = 0.f;
+      }
+    };
+
+    int buf = 0;
+    if (s0 < s1) stage(0, s0 + tid);
+    cp_async_commit();
+
+    for (int64_t sb = s0; sb < s1; sb += TILE) {
+      if (sb + TILE < s1) stage(buf ^ 1, sb + TILE + tid);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+
+      // Every pair of this warp's targets with this tile's sources is far
+      // (u >= 50) when the boxes are at least sqrt(50 (hs_t + hs_s)) apart;
+      // such tiles take the far limit with no per-pair test.  The boxes'
+      // distance is a lower bound of every pair's, so a far pair is never
+      // misclassified near; a pair within rounding of u = 50 may take the far
+      // limit, whose dropped terms are below 2e-9 there.
+      WarpBox sbox;
+      sbox.init();
+      for (int r = lane; r < NPR; r += 32) {
+        const float4 u = sP[buf][2 * r], v = sP[buf][2 * r + 1];
+        sbox.add(u.x, u.z, v.x, v.z);
+        sbox.add(u.y, u.w, v.y, v.w);
+      }
+      sbox.reduce();
+      const bool far_tile = all_far(tb, sbox);
+
+#pragma unroll 1
+      for (int g = 0; g < NPR; g += CG / 2) {
+        // per-lane partial sums over the group: .x even sources, .y odd
+        float2 sv[TPT][3], sd[TPT][3], sp[TPT][3];
+        float sdv[TPT][3];
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            sv[k][m] = make_float2(0.f, 0.f); sd[k][m] = make_float2(0.f, 0.f); sp[k][m] = make_float2(0.f, 0.f);
+            sdv[k][m] = 0.f;
+          }
+        }
+        if (far_tile) {
+#pragma unroll 2
+          for (int r = g; r < g + CG / 2; ++r) {
+            const float4 pa = sP[buf][2 * r], pb = sP[buf][2 * r + 1];
+            const float4 qa = sQ[buf][2 * r], qb = sQ[buf][2 * r + 1];
+            const float2 px = make_float2(pa.x, pa.y), py = make_float2(pa.z, pa.w), pz = make_float2(pb.x, pb.y);
+            const float2 ax = make_float2(qa.x, qa.y), ay = make_float2(qa.z, qa.w), az = make_float2(qb.x, qb.y);
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) {
+              // d = x_t - x_s (exact-rounded, as a subtraction)
+              const float2 dx = __ffma2_rn(px, M1, X[k][0]);
+              const float2 dy = __ffma2_rn(py, M1, X[k][1]);
+              const float2 dz = __ffma2_rn(pz, M1, X[k][2]);
+              float2 r2 = __fmul2_rn(dx, dx);
+              r2 = __ffma2_rn(dy, dy, r2);
+              r2 = __ffma2_rn(dz, dz, r2);
+              // far limit: q' = r^3, F' = -3 r^5 (the -3 is in AT3), no diffusion
+              const float2 ir = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
+              const float2 A = __fmul2_rn(ir, ir);
+              const float2 qq = __fmul2_rn(A, ir);
+              const float2 qA = __fmul2_rn(qq, A);
+              // w = alpha_s x d
+              const float2 wx = make_float2(ay.x * dz.x - az.x * dy.x, ay.y * dz.y - az.y * dy.y);
+              const float2 wy = make_float2(az.x * dx.x - ax.x * dz.x, az.y * dx.y - ax.y * dz.y);
+              const float2 wz = make_float2(ax.x * dy.x - ay.x * dx.x, ax.y * dy.y - ay.y * dx.y);
+              sv[k][0] = __ffma2_rn(qq, wx, sv[k][0]);
+              sv[k][1] = __ffma2_rn(qq, wy, sv[k][1]);
+              sv[k][2] = __ffma2_rn(qq, wz, sv[k][2]);
+              // F (alpha_t . w) d
+              float2 dot = __fmul2_rn(AT3[k][0], wx);
+              dot = __ffma2_rn(AT3[k][1], wy, dot);
+              dot = __ffma2_rn(AT3[k][2], wz, dot);
+              const float2 fd = __fmul2_rn(qA, dot);
+              sd[k][0] = __ffma2_rn(fd, dx, sd[k][0]);
+              sd[k][1] = __ffma2_rn(fd, dy, sd[k][1]);
+              sd[k][2] = __ffma2_rn(fd, dz, sd[k][2]);
+              sp[k][0] = __ffma2_rn(qq, ax, sp[k][0]);
+              sp[k][1] = __ffma2_rn(qq, ay, sp[k][1]);
+              sp[k][2] = __ffma2_rn(qq, az, sp[k][2]);
+            }
+          }
+        } else {
+          // Tiles with possible near pairs: scalar, one source at a time,
+          // accumulated into lane .x.
+          auto one = [&](float sx, float sy, float sz, float shs, float qx, float qy, float qz, float qv) {
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) {
+              const float dx = xt[k][0] - sx, dy = xt[k][1] - sy, dz = xt[k][2] - sz;
+              const float r2 = dx * dx + dy * dy + dz * dz;
+              // far test r^2 >= 50 (hs_t + hs_s) as one FMA against the
+              // target's precomputed 50 hs_t
+              const bool near = fmaf(-kFarU, shs, r2) < h50[k];
+              const float ir = fast_rsqrt(r2);
+              const float A = ir * ir;
+              float qq = A * ir;
+              float FF = -3.0f * qq * A;
+              // the full formula only when some lane of the warp needs it:
+              // the vote keeps the common all-far case free of divergence
+              if (__any_sync(0xffffffffu, near)) {
+                if (near) {
+                  const PairTerms<float> pt = pair_terms_near(r2, hst[k] + shs);
+                  qq = pt.q; FF = pt.F;
+                  // v_t a_s - v_s a_t per pair, so nearly equal strengths cancel
+                  // before they are summed (as in DIFFUSION, interaction_utils.h:358-369)
+                  sdv[k][0] += pt.zd * (vt[k] * qx - qv * at[k][0]);
+                  sdv[k][1] += pt.zd * (vt[k] * qy - qv * at[k][1]);
+                  sdv[k][2] += pt.zd * (vt[k] * qz - qv * at[k][2]);
+                  ++nfull;
+                }
+              }
+              const float wx = qy * dz - qz * dy;
+              const float wy = qz * dx - qx * dz;
+              const float wz = qx * dy - qy * dx;
+              sv[k][0].x += qq * wx; sv[k][1].x += qq * wy; sv[k][2].x += qq * wz;
+              const float fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
+              sd[k][0].x += fd * dx; sd[k][1].x += fd * dy; sd[k][2].x += fd * dz;
+              sp[k][0].x += qq * qx; sp[k][1].x += qq * qy; sp[k][2].x += qq * qz;
+            }
+          };
+#pragma unroll 1
+          for (int r = g; r < g + CG / 2; ++r) {
+            const float4 pa = sP[buf][2 * r], pb = sP[buf][2 * r + 1];
+            const float4 qa = sQ[buf][2 * r], qb = sQ[buf][2 * r + 1];
+            one(pa.x, pa.z, pb.x, pb.z, qa.x, qa.z, qb.x, qb.z);
+            one(pa.y, pa.w, pb.y, pb.w, qa.y, qa.w, qb.y, qb.w);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+          float svs[3], sds[3], sps[3];
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            svs[m] = sv[k][m].x + sv[k][m].y;
+            sds[m] = sd[k][m].x + sd[k][m].y;
+            sps[m] = sp[k][m].x + sp[k][m].y;
+          }
+          // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t)
+          const float ex = at[k][1] * sps[2] - at[k][2] * sps[1] + sds[0] + a.nu2 * sdv[k][0];
+          const float ey = at[k][2] * sps[0] - at[k][0] * sps[2] + sds[1] + a.nu2 * sdv[k][1];
+          const float ez = at[k][0] * sps[1] - at[k][1] * sps[0] + sds[2] + a.nu2 * sdv[k][2];
+          two_sum_acc(vh[k][0], vl[k][0], svs[0]);
+          two_sum_acc(vh[k][1], vl[k][1], svs[1]);
+          two_sum_acc(vh[k][2], vl[k][2], svs[2]);
+          two_sum_acc(dh[k][0], dl[k][0], ex);
+          two_sum_acc(dh[k][1], dl[k][1], ey);
+          two_sum_acc(dh[k][2], dl[k][2], ez);
+        }
+      }
+      __syncthreads();
+      buf ^= 1;
+    }
+    cp_async_wait<0>();
+    const unsigned wsum = __reduce_add_sync(0xffffffffu, nfull);
+    if (lane == 0 && wsum) atomicAdd(a.nfull, (unsigned long long)wsum);
+
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      const int64_t ti = t0 + tid + k * BLOCK;
+      if (ti < tend) {
+        double *o = a.partial + (int64_t)c * 6 * a.cap + ti;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          o[m * a.cap] = ((double)vh[k][m] + (double)vl[k][m]) * kInv4Pi;
+          o[(3 + m) * a.cap] = ((double)dh[k][m] + (double)dl[k][m]) * kInv4Pi;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace pgpu
