@@ -238,8 +238,11 @@ int pgpu_surrogate_set_mlp(pgpu_ctx *ctx, pgpu_mlp *mlp);
 int pgpu_get_stream(pgpu_ctx *ctx, void **stream);
 
 /* Measures the device's sustained FP32 FMA throughput (TFLOP/s, an FMA
- * counted as 2 flops) with a register-resident FFMA loop on every SM, for
- * roofline denominators.  No PAWAN counterpart. */
+ * counted as 2 flops) with register-resident FMA loops on every SM, for
+ * roofline denominators: scalar FFMA and the packed two-wide FFMA2 of sm_100.
+ * pgpu_fp32_peak gives the larger of the two (ms is set to 0).  No PAWAN
+ * counterpart. */
+int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops);
 int pgpu_fp32_peak(int device, double *tflops, double *ms);
 
 /* Largest system pgpu_rates_noalloc accepts (its fixed scratch: ~13.6 MB of

@@ -32,7 +32,7 @@ EXPORTS = [
     "pgpu_get_states_flat", "pgpu_get_rates_flat", "pgpu_solve", "pgpu_get_rates", "pgpu_step",
     "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
     "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
-    "pgpu_fp32_peak", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
+    "pgpu_fp32_peak", "pgpu_fp32_peaks", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
     "pgpu_surrogate_disable", "pgpu_surrogate_get_stats", "pgpu_surrogate_tree", "pgpu_mlp_num_params",
     "pgpu_mlp_create", "pgpu_mlp_destroy", "pgpu_mlp_last_error", "pgpu_mlp_get_params", "pgpu_mlp_set_params",
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
@@ -117,6 +117,7 @@ def load(build_if_missing: bool = False):
         "pgpu_version": (C.c_char_p, []),
         "pgpu_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
         "pgpu_fp32_peak": (C.c_int, [C.c_int, _dp, _dp]),
+        "pgpu_fp32_peaks": (C.c_int, [C.c_int, _dp, _dp]),
         "pgpu_pair_counts": (C.c_int, [vp, _i64p, _i64p]),
         "pgpu_surrogate_config_default": (None, [C.POINTER(SurrogateConfig)]),
         "pgpu_surrogate_enable": (C.c_int, [vp, C.c_int32, C.POINTER(SurrogateConfig)]),
@@ -158,8 +159,19 @@ def _c(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def fp32_peaks(device: int = 0) -> tuple[float, float]:
+    """Measured FP32 FMA throughput in TFLOP/s: (scalar FFMA loop, packed FFMA2 loop)."""
+    lib = load()
+    f1, f2 = C.c_double(), C.c_double()
+    rc = lib.pgpu_fp32_peaks(device, C.byref(f1), C.byref(f2))
+    if rc != PGPU_OK:
+        raise PgpuError(rc, "pgpu_fp32_peaks failed")
+    return f1.value, f2.value
+
+
 def fp32_peak(device: int = 0) -> float:
-    """Measured FP32 FMA throughput of the device in TFLOP/s."""
+    """Measured FP32 FMA throughput of the device in TFLOP/s (the larger of
+    the scalar and packed loops)."""
     lib = load()
     tf, ms = C.c_double(), C.c_double()
     rc = lib.pgpu_fp32_peak(device, C.byref(tf), C.byref(ms))

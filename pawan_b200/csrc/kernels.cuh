@@ -734,4 +734,23 @@ static __global__ void __launch_bounds__(256) ffma_peak_kernel(float *out, int i
   if (s == -1.2345e30f) *out = s;
 }
 
+// The same probe with the packed two-wide FMA of sm_100 (__ffma2_rn): each
+// instruction does two FP32 FMAs.
+static __global__ void __launch_bounds__(256) ffma2_peak_kernel(float *out, int iters, float a, float b) {
+  float2 x[kFfmaChains / 2];
+  const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+#pragma unroll
+  for (int k = 0; k < kFfmaChains / 2; ++k) x[k] = make_float2(threadIdx.x * 1e-3f + 2 * k, threadIdx.x * 1e-3f + 2 * k + 1);
+  for (int i = 0; i < iters; i += 4) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int k = 0; k < kFfmaChains / 2; ++k) x[k] = __ffma2_rn(x[k], a2, b2);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < kFfmaChains / 2; ++k) s += x[k].x + x[k].y;
+  if (s == -1.2345e30f) *out = s;
+}
+
 }  // namespace pgpu
