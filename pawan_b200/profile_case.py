@@ -23,8 +23,9 @@ def main() -> None:
     ap.add_argument("--fp64", action="store_true")
     ap.add_argument("--block", type=int, default=0, help="pair-kernel block size (0: library default)")
     ap.add_argument("--tpt", type=int, default=0, help="targets per thread (0: library default)")
+    ap.add_argument("--sigma", type=float, default=0.02, help="smoothing radius (smaller: fewer near pairs)")
     a = ap.parse_args()
-    w = cases.ring_gaussian(stations=a.stations, per_section=1000, sigma=0.02, seed=1)
+    w = cases.ring_gaussian(stations=a.stations, per_section=1000, sigma=a.sigma, seed=1)
     c = capi.Context(precision=capi.FP64 if a.fp64 else capi.FP32C, nu=1e-4, block=a.block, tpt=a.tpt)
     k = c.add_wake(w.n)
     c.set_particles(k, w)
