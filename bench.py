@@ -327,11 +327,15 @@ def run_ours(args):
         fp32_peak = max(ffma_peak, ffma2_peak)
         flops_per_launch = (FLOPS_PER_PAIR * full_timed + FLOPS_PER_FAR_PAIR * (pairs_timed - full_timed)) / max(pair_launches, 1)
         achieved = flops_per_launch / (pair_avg_ms * 1e-3) / 1e12
+        # DRAM bytes of one pair-kernel launch at this size, from the ncu
+        # capture summarised in profiles/ (a line "traffic_bytes_per_launch[N=..., ...] = B")
         traffic = None
-        tf = ROOT / "profiles" / "pair_kernel_traffic.json"
+        tf = ROOT / "profiles" / "pair_kernel_ring1M_dram.md"
         if tf.exists():
-            tj = json.loads(tf.read_text())
-            traffic = tj.get("bytes_per_launch_at", {}).get(str(n))
+            import re
+            for m in re.finditer(r"traffic_bytes_per_launch\[N=(\d+)[^\]]*\]\s*=\s*(\d+)", tf.read_text()):
+                if int(m.group(1)) == n:
+                    traffic = int(m.group(2))
         cpu = None
         from oracle import oracle as O
         if O.ref_available():

@@ -155,7 +155,8 @@ int pgpu_kernel_shapes(int *block, int *tpt, int max);
  *
  * With the surrogate enabled, every rate evaluation of the context's single
  * system uses an octree: each target leaf's near field (cells closer than
- * near_widths cube widths) is summed exactly with the direct kernel's terms,
+ * near_widths cube widths, or with a particle within 4 sigma_ij of the leaf's)
+ * is summed exactly with the direct kernel's terms,
  * and farther cells act through their multipole moments (order 0/1/2),
  * optionally corrected by the learned model of pgpu_surrogate_set_mlp.  After
  * every evaluation, check_targets sampled targets are recomputed by the direct
@@ -163,9 +164,9 @@ int pgpu_kernel_shapes(int *block, int *tpt, int max);
  * evaluation is redone by the direct sum (the surrogate never returns an
  * unchecked result when check_targets > 0). */
 typedef struct pgpu_surrogate_config {
-  int leaf_size;       /* particles per octree leaf, 1..512 (default 512) */
+  int leaf_size;       /* particles per octree leaf, 1..512 (default 256) */
   double near_widths;  /* near field: cells closer than this many cube widths (default 4) */
-  int order;           /* far-field expansion: 0 monopole, 1 + dipole (default), 2 + quadrupole */
+  int order;           /* far-field expansion: 0 monopole, 1 + dipole, 2 + quadrupole (default) */
   int use_mlp;         /* add the learned correction to the order-1 far field (pgpu_surrogate_set_mlp) */
   double tolerance;    /* maximum relative velocity error on the sampled targets (default 1e-4) */
   int check_targets;   /* targets re-checked by the direct sum per evaluation (default 4096, 0 = off) */

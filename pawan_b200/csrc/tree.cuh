@@ -12,8 +12,9 @@
 //   5. per-cell moments about the particle centroid (moments_kernel)
 //   6. per target leaf, the interaction lists (lists_kernel): a source cell
 //      whose centroid is at least `near_widths` cube widths beyond the target
-//      leaf's bounding sphere is far (evaluated from its moments); a leaf that
-//      is not far is near (exact pair sum).
+//      leaf's bounding sphere, and whose particles are all at least 4 sigma_ij
+//      from the leaf's, is far (evaluated from its moments); a leaf that is not
+//      far is near (exact pair sum).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -23,6 +24,13 @@ namespace pgpu {
 constexpr int kTreeLevels = 21;
 constexpr int kCellFloats = 40;
 constexpr int kListStack = 256;
+// Smallest u = rho^2 / sigma_ij^2 between any particle of a far cell and any
+// of the target leaf (rho >= 4 sigma_ij).  At 4M particles on the coaxial
+// rings, u >= 16 / 25 / 36 give the same sampled error (1.4-1.8e-5) and cost
+// 846 / 1022 / 1168 ms per evaluation with 256-particle leaves; without the
+// test, 128-particle leaves put cells within ~2 sigma in the far field and the
+// error grows to 7.5e-3.
+constexpr float kFarAccept = 16.f;
 
 struct TreeCell {
   int start, end;       // sorted particle range
@@ -36,7 +44,8 @@ struct TreeCell {
 // Per-cell data (floats), about the cell's particle centroid c, y = x - c:
 //   0-2 c, 3-5 A = sum alpha, 6-14 M[a][b] = sum alpha_a y_b,
 //   15-32 Q[a][bc] = sum alpha_a y_b y_c for bc in (00,01,02,11,12,22),
-//   33 R = max |y|, 34 w = cube width, 35-37 cube centre, 38 mean sigma^2/2, 39 count.
+//   33 R = max |y|, 34 w = cube width, 35-37 cube centre, 38 mean sigma^2/2,
+//   39 largest sigma^2/2.
 struct CellData { float v[kCellFloats]; };
 
 __device__ __forceinline__ unsigned f2ord(float f) {
@@ -210,9 +219,10 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
     const double cx = t[0] / cnt, cy = t[1] / cnt, cz = t[2] / cnt;
     double m[27];
     for (int k = 0; k < 27; ++k) m[k] = 0.0;
-    float R = 0.f;
+    float R = 0.f, H = 0.f;
     for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
       const float4 p = Ps[i], q = Qs[i];
+      H = fmaxf(H, p.w);
       const double y[3] = {p.x - cx, p.y - cy, p.z - cz};
       const double a[3] = {q.x, q.y, q.z};
       R = fmaxf(R, (float)sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]));
@@ -229,6 +239,7 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
     double mt[27];
     for (int k = 0; k < 27; ++k) mt[k] = block_sum_d(m[k], red);
     const float Rm = block_max_f(R, redf);
+    const float Hm = block_max_f(H, redf);
     if (threadIdx.x == 0) {
       CellData d;
       d.v[0] = (float)cx; d.v[1] = (float)cy; d.v[2] = (float)cz;
@@ -243,7 +254,7 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
       d.v[36] = geo[1] + (iy + 0.5f) * w;
       d.v[37] = geo[2] + (iz + 0.5f) * w;
       d.v[38] = (float)(t[6] / cnt);
-      d.v[39] = (float)cnt;
+      d.v[39] = Hm;
       out[ci] = d;
     }
     __syncthreads();
@@ -264,7 +275,7 @@ __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const in
   if (li >= nleaves) return;
   const int T = leaves[li];
   const TreeCell tc = cells[T];
-  const float tx = cd[T].v[0], ty = cd[T].v[1], tz = cd[T].v[2], tR = cd[T].v[33];
+  const float tx = cd[T].v[0], ty = cd[T].v[1], tz = cd[T].v[2], tR = cd[T].v[33], tH = cd[T].v[39];
   int stack[kListStack];
   int sp = 0;
   stack[sp++] = 0;
@@ -276,7 +287,12 @@ __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const in
     const bool contains = c.start <= tc.start && tc.end <= c.end;
     const float dx = cd[ci].v[0] - tx, dy = cd[ci].v[1] - ty, dz = cd[ci].v[2] - tz;
     const float d = sqrtf(dx * dx + dy * dy + dz * dz) - tR;
-    if (!contains && d >= near_widths * cd[ci].v[34]) {
+    // far: beyond near_widths cube widths, and every pair of the two cells at
+    // u = rho^2 / sigma_ij^2 >= kFarAccept, so that the Gaussian regularisation
+    // the singular-kernel expansion leaves out stays small
+    const float gap = d - cd[ci].v[33];
+    if (!contains && d >= near_widths * cd[ci].v[34] && gap > 0.f &&
+        gap * gap >= kFarAccept * (tH + cd[ci].v[39])) {
       if (pass) far_list[fo + nf] = ci;
       ++nf;
     } else if (c.nchild == 0) {

@@ -1,6 +1,8 @@
 """A small, self-contained workload for profilers (ncu) and quick timing.
 
     python -m pawan_b200.profile_case [--stations 200] [--solves 3] [--fp64] [--steps 1] [--block 256 --tpt 2]
+    python -m pawan_b200.profile_case --surrogate 200000 [--solves 2]
+    python -m pawan_b200.profile_case --mlp-train 20
 
 Builds the Gaussian-core vortex ring of the 1M-particle benchmark with
 ``stations`` x 1000 particles (200 -> N = 200,000), runs ``solves`` rate
@@ -24,7 +26,17 @@ def main() -> None:
     ap.add_argument("--block", type=int, default=0, help="pair-kernel block size (0: library default)")
     ap.add_argument("--tpt", type=int, default=0, help="targets per thread (0: library default)")
     ap.add_argument("--sigma", type=float, default=0.02, help="smoothing radius (smaller: fewer near pairs)")
+    ap.add_argument("--surrogate", type=int, default=0,
+                    help="instead: octree far field (order 2) on two coaxial rings of this many particles")
+    ap.add_argument("--mlp-train", type=int, default=0,
+                    help="instead: this many training steps of the far-field network (batch 65536)")
     a = ap.parse_args()
+    if a.surrogate:
+        surrogate_case(a.surrogate, a.solves)
+        return
+    if a.mlp_train:
+        mlp_case(a.mlp_train)
+        return
     w = cases.ring_gaussian(stations=a.stations, per_section=1000, sigma=a.sigma, seed=1)
     c = capi.Context(precision=capi.FP64 if a.fp64 else capi.FP32C, nu=1e-4, block=a.block, tpt=a.tpt)
     k = c.add_wake(w.n)
@@ -42,6 +54,32 @@ def main() -> None:
     d, vbi = c.diagnose(0)
     print("diagnostics", d.tolist(), "vbi", vbi.tolist())
     c.close()
+
+
+def surrogate_case(n: int, solves: int) -> None:
+    w = cases.leapfrog_rings(n_total=n)
+    c = capi.Context(precision=capi.FP32C, nu=1e-4)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    c.surrogate_enable(order=2, tolerance=1e-4, check_targets=4096)
+    for _ in range(solves):
+        c.solve()
+    c.sync()
+    st = c.surrogate_stats()
+    print(f"N {w.n} surrogate: tree {st['ms_tree']:.2f} ms, eval {st['ms_eval']:.2f} ms, check {st['ms_check']:.2f} ms, "
+          f"sampled error {st['last_err_vel']:.2e}, fallbacks {st['fallbacks']}")
+    c.close()
+
+
+def mlp_case(steps: int) -> None:
+    import numpy as np
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(262144, 24)).astype(np.float32)
+    t = np.tanh(x[:, :6]).astype(np.float32)
+    m = capi.Mlp(seed=1)
+    m.set_dataset(x, t)
+    hist = m.train(steps, batch=65536, lr=1e-3, seed=2)
+    print(f"MLP {steps} training steps of batch 65536: loss {hist[0]:.4f} -> {hist[-1]:.4f}")
 
 
 if __name__ == "__main__":

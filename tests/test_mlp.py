@@ -78,11 +78,17 @@ def test_training_reduces_loss(gpu):
     assert hist[-20:].mean() < 0.1 * hist[:5].mean()
 
 
+# Leaf size of the octree for the systems of 20k particles and more, in
+# training and in evaluation alike: the network is trained on the cells of
+# one leaf size and does not carry over to another.
+LEAF = 256
+
+
 def surrogate_rates(w, order, mlp=None):
     c = capi.Context(precision=capi.FP32C, nu=1e-4)
     k = c.add_wake(w.n)
     c.set_particles(k, w)
-    c.surrogate_enable(order=order, use_mlp=1 if mlp is not None else 0, check_targets=0)
+    c.surrogate_enable(order=order, use_mlp=1 if mlp is not None else 0, check_targets=0, leaf_size=LEAF)
     if mlp is not None:
         c.surrogate_set_mlp(mlp)
     c.solve()
@@ -102,7 +108,7 @@ def training_set(mlp, n_per_case=200_000):
         c.set_particles(k, w)
         # the 5000-particle ring has far cells only with small leaves; the
         # features are scale-free, so samples of any leaf size mix
-        c.surrogate_enable(order=1, check_targets=0, leaf_size=32 if w.n < 20_000 else 512)
+        c.surrogate_enable(order=1, check_targets=0, leaf_size=32 if w.n < 20_000 else LEAF)
         c.solve()
         mlp.add_samples(c, n_per_case, seed=i)
         c.close()
