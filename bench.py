@@ -12,13 +12,14 @@ updates.  Synthetic seeded data (no dataset is involved).
 
 With --gpus N > 1 (torchrun, one rank per GPU) every rank advances its own
 copy of the ring (independent replicas, weak scaling; the step has no
-collective, see DESIGN.md).
+collective).
 
 `value` is RK4 steps/s with the particles resident in HBM (CUDA events on the
 library's stream, max over ranks); `e2e` is the same metric through the C ABI
 with host buffers: each step uploads the particles from pinned host memory,
 steps, and downloads the new state.  `roofline` rates the pair kernel against
-the FP32 FMA peak measured on the same GPU; `cpu_baseline` times PAWAN's own
+the FP32 FMA peak measured on the same GPU (the larger of a scalar FFMA and a
+packed FFMA2 register loop); `cpu_baseline` times PAWAN's own
 OpenMP code (compiled from its sources) on the host cores on a bounded sample
 and extrapolates quadratically to N.
 
@@ -26,6 +27,11 @@ and extrapolates quadratically to N.
 host cores with all threads: each step is one RK4 step of a random
 SAMPLE_N-particle subset of the same ring, and the reported steps/s is
 extrapolated to N by the ratio of pair counts.
+
+The `surrogate` object times configuration 5 on rank 0: two coaxial rings of
+4M particles, one RK4 step with the octree far field (quadrupole order,
+sampled direct-sum check of 4096 targets per evaluation) against the plain
+direct-sum RK4 step.
 """
 from __future__ import annotations
 
