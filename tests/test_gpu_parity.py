@@ -322,3 +322,39 @@ def test_ring1m_stretching_and_diffusion_sum_to_zero(gpu, ring1m_rates):
     scale = np.abs(a).sum(axis=0).max()
     print(f"1M ring: |sum dalpha/dt| / sum |dalpha/dt| = {tot / scale:.2e}")
     assert tot <= 1e-6 * scale
+
+
+def test_config3_64_uneven_rings_batched_sampled(gpu):
+    """Configuration 3 at full size: 64 independent rings, N log-uniform in
+    [2e3, 2e5] (seed 2), as 64 systems of one context evaluated in one
+    persistent launch; 64 seeded targets of the three smallest and three
+    largest rings against the FP64 restatement of each ring alone."""
+    ws = cases.uneven_rings(count=64, nmin=2e3, nmax=2e5, seed=2)
+    c, ids = ctx_with(ws, capi.FP32C, 1e-4, systems=list(range(len(ws))))
+    c.solve()
+    order = np.argsort([w.n for w in ws])
+    rng = np.random.default_rng(3)
+    worst = 0.0
+    for i in list(order[:3]) + list(order[-3:]):
+        w = ws[i]
+        v, a = c.rates(ids[i])
+        rows = np.sort(rng.choice(w.n, 64, replace=False))
+        vr, ar = O.restate_rates(w, 1e-4, targets=rows)
+        worst = max(worst, O.rel_err(v[rows], vr), O.rel_err(a[rows], ar))
+    c.close()
+    print(f"64 rings, {sum(w.n for w in ws)} particles: worst sampled error {worst:.2e}")
+    assert worst < TOL[capi.FP32C]
+
+
+def test_conservation_and_fp32c_trajectory(gpu):
+    """Ten RK4 steps of a 20k ring in both modes: total vorticity stays at
+    rounding level and the FP32C trajectory follows the FP64 one within the
+    FP32C gate."""
+    from pawan_b200 import conservation
+    res = conservation.run(stations=20, steps=10, every=5)
+    last = res["records"][-1]
+    print(conservation.markdown(res))
+    assert last["fp64"]["total vorticity"] < 1e-13
+    assert last["fp32c"]["total vorticity"] < 1e-9
+    assert last["fp32c_vs_fp64"]["displacement"] < TOL[capi.FP32C]
+    assert last["fp32c_vs_fp64"]["alpha"] < TOL[capi.FP32C]
