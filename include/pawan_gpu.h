@@ -110,6 +110,29 @@ int pgpu_get_rates(pgpu_ctx *ctx, int32_t wake, double *vel, double *dalpha);
  * step.  The state stays on the device. */
 int pgpu_step(pgpu_ctx *ctx, int scheme, double dt, int32_t nsteps);
 
+/* ---------------------------------------------------------------------------
+ * One system over several GPUs (no PAWAN counterpart: PAWAN runs on one host).
+ * Each GPU's context holds the whole system and owns a contiguous range of
+ * its targets; all particles stay sources.  A step then runs stage by stage:
+ * pgpu_stage evaluates the owned targets' rates from the current source
+ * records of all particles and updates the owned particles (state and
+ * records); before the next stage the caller copies the other GPUs' owned
+ * records into this context's record arrays (an all-gather), ordered on the
+ * context's stream (pgpu_get_stream).
+ *
+ * pgpu_set_target_range: targets [first, first + count) of the system (in
+ * the order of its wakes' particles); count < 0 restores all targets.  While
+ * any system has a range, pgpu_step and pgpu_diagnose refuse (the state of
+ * the other targets is not advanced here), and the surrogate is off.
+ * pgpu_stage: stage 0..3 (RK4), 0..2 (RK3) or 0 (Euler) of one step of every
+ * system; the last stage finishes the step (and applies vinf).
+ * pgpu_records: device pointers to the system's source records, one per
+ * particle in system order: FP32C float4 (x, y, z, sigma^2/2) and
+ * (alpha_x, alpha_y, alpha_z, vol); FP64 mode double4. */
+int pgpu_set_target_range(pgpu_ctx *ctx, int32_t system, int64_t first, int64_t count);
+int pgpu_stage(pgpu_ctx *ctx, int scheme, int stage, double dt);
+int pgpu_records(pgpu_ctx *ctx, int32_t system, void **P, void **Q);
+
 /* Replaces: __interaction::diagnose (interaction.cpp:64-194) for one system.
  * out[15] = total vorticity(3), linear impulse(3), angular impulse(3),
  * helicity, enstrophy, enstrophyF, kinetic energy, kinetic energyF, Zc - the

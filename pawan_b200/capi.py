@@ -37,7 +37,7 @@ EXPORTS = [
     "pgpu_mlp_create", "pgpu_mlp_destroy", "pgpu_mlp_last_error", "pgpu_mlp_get_params", "pgpu_mlp_set_params",
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
-    "pgpu_rates_noalloc", "pgpu_noalloc_last_error",
+    "pgpu_rates_noalloc", "pgpu_noalloc_last_error", "pgpu_set_target_range", "pgpu_stage", "pgpu_records",
 ]
 
 
@@ -142,6 +142,9 @@ def load(build_if_missing: bool = False):
                                           C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int64, _i64p, _i64p, _i64p]),
         "pgpu_rates_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int64, C.c_double, vp, vp, vp]),
         "pgpu_noalloc_last_error": (C.c_char_p, []),
+        "pgpu_set_target_range": (C.c_int, [vp, C.c_int32, C.c_int64, C.c_int64]),
+        "pgpu_stage": (C.c_int, [vp, C.c_int, C.c_int, C.c_double]),
+        "pgpu_records": (C.c_int, [vp, C.c_int32, C.POINTER(vp), C.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -322,6 +325,20 @@ class Context:
         return p.value, f.value
 
     # ------------------------------------------------------------ far-field surrogate
+    # ------------------------------------------------------------ sharding
+    def set_target_range(self, system: int, first: int, count: int):
+        """Owned targets [first, first + count) of the system; count < 0 restores all."""
+        self._ck(self.lib.pgpu_set_target_range(self.h, system, int(first), int(count)))
+
+    def stage(self, scheme: str, stage: int, dt: float):
+        self._ck(self.lib.pgpu_stage(self.h, SCHEMES[scheme], int(stage), float(dt)))
+
+    def records(self, system: int = 0) -> tuple[int, int]:
+        """Device addresses of the system's source records P and Q."""
+        P, Q = C.c_void_p(), C.c_void_p()
+        self._ck(self.lib.pgpu_records(self.h, system, C.byref(P), C.byref(Q)))
+        return P.value, Q.value
+
     def surrogate_enable(self, system: int = 0, **kw):
         cfg = SurrogateConfig()
         self.lib.pgpu_surrogate_config_default(C.byref(cfg))

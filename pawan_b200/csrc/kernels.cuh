@@ -38,10 +38,12 @@ constexpr int kDiagFields = 19;
 // One system in the work list (sorted by decreasing work).
 struct PlanEntry {
   int64_t off;         // first particle slot of the system
-  int64_t n;           // particles in the system
+  int64_t n;           // particles in the system (all of them are sources)
   int64_t item_start;  // first work item of the system
   int64_t tiles;       // target tiles
   int64_t chunk;       // sources per chunk (multiple of the source tile)
+  int64_t toff;        // targets: particles [off + toff, off + toff + tn) of the system
+  int64_t tn;
 };
 
 template <typename T> struct PairArgs {
@@ -188,10 +190,10 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
     const int64_t local = item - pe.item_start;
     const int64_t tile = local / a.nch;
     const int c = (int)(local - tile * a.nch);
-    const int64_t t0 = pe.off + tile * TT;
-    const int64_t tend = pe.off + pe.n;
+    const int64_t t0 = pe.off + pe.toff + tile * TT;
+    const int64_t tend = pe.off + pe.toff + pe.tn;  // end of the targets
     const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
-    const int64_t s1 = min(s0 + pe.chunk, tend);
+    const int64_t s1 = min(s0 + pe.chunk, pe.off + pe.n);
 
     T xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT], h50[TPT];
     T vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
@@ -411,6 +413,7 @@ struct StageArgs {
   void *Q;
   const int64_t *sys_off;  // [nsys + 1] ascending slot offsets (capacity layout)
   const int64_t *sys_n;    // [nsys]
+  const int64_t *sys_t;    // [2 nsys] owned particles [sys_t[2s], sys_t[2s+1]) of each system
   int nsys;
   int nch;
   int64_t cap;
@@ -435,7 +438,8 @@ template <typename T>
 __global__ void stage_kernel(StageArgs a) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.cap; i += (int64_t)gridDim.x * blockDim.x) {
     const int s = find_sys(a.sys_off, a.nsys, i);
-    if (i - a.sys_off[s] >= a.sys_n[s]) continue;
+    const int64_t li = i - a.sys_off[s];
+    if (li >= a.sys_n[s] || li < a.sys_t[2 * s] || li >= a.sys_t[2 * s + 1]) continue;
     double k[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) {

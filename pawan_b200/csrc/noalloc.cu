@@ -81,11 +81,15 @@ __global__ void noalloc_pack_kernel(const double *pos, const double *alpha, cons
     plan[0].item_start = 0;
     plan[0].tiles = tiles;
     plan[0].chunk = (per + kNoAllocBlock - 1) / kNoAllocBlock * kNoAllocBlock;
+    plan[0].toff = 0;
+    plan[0].tn = n;
     plan[1].off = 0;
     plan[1].n = 0;
     plan[1].item_start = tiles * nch;
     plan[1].tiles = 0;
     plan[1].chunk = 0;
+    plan[1].toff = 0;
+    plan[1].tn = 0;
   }
 }
 

@@ -58,10 +58,10 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
     const int64_t local = item - pe.item_start;
     const int64_t tile = local / a.nch;
     const int c = (int)(local - tile * a.nch);
-    const int64_t t0 = pe.off + tile * TT;
-    const int64_t tend = pe.off + pe.n;
+    const int64_t t0 = pe.off + pe.toff + tile * TT;
+    const int64_t tend = pe.off + pe.toff + pe.tn;  // end of the targets
     const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
-    const int64_t s1 = min(s0 + pe.chunk, tend);
+    const int64_t s1 = min(s0 + pe.chunk, pe.off + pe.n);
 
     // targets: scalar copies for the near path and the fold, duplicated
     // float2 copies for the packed far loop

@@ -16,6 +16,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <map>
 #include <string>
 #include <tuple>
@@ -59,6 +60,7 @@ struct SysRec {
   std::vector<int> wakes;
   int64_t off = 0, cap = 0;
   double zc = 0.0;  // last reported Zc (PAWAN keeps _Zc across calls)
+  int64_t t_first = 0, t_count = -1;  // owned targets (pgpu_set_target_range); count < 0: all
 };
 
 }  // namespace
@@ -76,7 +78,7 @@ struct pgpu_ctx {
   double *x0 = nullptr, *acc = nullptr, *rates = nullptr, *sig = nullptr, *vol = nullptr;
   double *partial = nullptr, *stage = nullptr, *d_diag = nullptr;
   void *P = nullptr, *Q = nullptr;
-  int64_t *d_sysoff = nullptr, *d_sysn = nullptr;
+  int64_t *d_sysoff = nullptr, *d_sysn = nullptr, *d_syst = nullptr;
   PlanEntry *d_plan = nullptr, *d_plan_diag = nullptr;
   unsigned int *d_counters = nullptr;
   unsigned long long *d_nfull = nullptr;
@@ -181,6 +183,7 @@ int freeze(pgpu_ctx *c) {
   const size_t ns = c->sys.size();
   if ((r = alloc((void **)&c->d_sysoff, (ns + 1) * sizeof(int64_t)))) return r;
   if ((r = alloc((void **)&c->d_sysn, ns * sizeof(int64_t)))) return r;
+  if ((r = alloc((void **)&c->d_syst, 2 * ns * sizeof(int64_t)))) return r;
   if ((r = alloc((void **)&c->d_plan, (ns + 1) * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_plan_diag, 2 * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_counters, 4 * sizeof(unsigned int)))) return r;
@@ -205,24 +208,49 @@ int freeze(pgpu_ctx *c) {
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// Work list: systems by decreasing size, target tiles x source chunks each.
-std::vector<PlanEntry> build_plan(const pgpu_ctx *c, const std::vector<int> &systems, int shape, int nch) {
+// Owned targets [first, first + count) of system s (all of them unless
+// pgpu_set_target_range restricted it), clamped to its particles.
+std::pair<int64_t, int64_t> owned(const pgpu_ctx *c, int s) {
+  const int64_t n = sys_n(c, s);
+  const SysRec &S = c->sys[s];
+  if (S.t_count < 0) return {0, n};
+  const int64_t lo = std::min(S.t_first, n);
+  return {lo, std::min(S.t_count, n - lo)};
+}
+
+bool restricted(const pgpu_ctx *c) {
+  for (const SysRec &S : c->sys)
+    if (S.t_count >= 0) return true;
+  return false;
+}
+
+// Work list: systems by decreasing work, target tiles x source chunks each.
+// With own_targets, only each system's owned targets are listed (all
+// particles stay sources); otherwise every particle is a target.
+std::vector<PlanEntry> build_plan(const pgpu_ctx *c, const std::vector<int> &systems, int shape, int nch,
+                                  bool own_targets = true) {
   const int64_t TT = (int64_t)kShapes[shape].block * kShapes[shape].tpt;
   const int64_t TILE = kShapes[shape].block;
   std::vector<std::pair<int64_t, int>> order;
-  for (int s : systems) order.push_back({sys_n(c, s), s});
+  for (int s : systems) {
+    const int64_t tn = own_targets ? owned(c, s).second : sys_n(c, s);
+    order.push_back({tn * sys_n(c, s), s});
+  }
   std::stable_sort(order.begin(), order.end(), [](auto &a, auto &b) { return a.first > b.first; });
   std::vector<PlanEntry> plan;
   int64_t item = 0;
   for (auto &o : order) {
-    const int64_t n = o.first;
-    if (n <= 0) continue;
+    const int64_t n = sys_n(c, o.second);
+    const auto t = own_targets ? owned(c, o.second) : std::make_pair<int64_t, int64_t>(0, sys_n(c, o.second));
+    if (n <= 0 || t.second <= 0) continue;
     PlanEntry e;
     e.off = c->sys[o.second].off;
     e.n = n;
     e.item_start = item;
-    e.tiles = ceil_div(n, TT);
+    e.tiles = ceil_div(t.second, TT);
     e.chunk = ceil_div(ceil_div(n, nch), TILE) * TILE;
+    e.toff = t.first;
+    e.tn = t.second;
     item += e.tiles * nch;
     plan.push_back(e);
   }
@@ -236,7 +264,7 @@ int choose_nch(const pgpu_ctx *c, int shape) {
   if (c->cfg.chunks > 0) return std::min(c->cfg.chunks, kMaxChunks);
   const int64_t TT = (int64_t)kShapes[shape].block * kShapes[shape].tpt;
   int64_t tiles = 0;
-  for (size_t s = 0; s < c->sys.size(); ++s) tiles += ceil_div(sys_n(c, (int)s), TT);
+  for (size_t s = 0; s < c->sys.size(); ++s) tiles += ceil_div(owned(c, (int)s).second, TT);
   if (tiles <= 0) return 1;
   const int64_t want = 24LL * c->grid[shape];
   return (int)std::max<int64_t>(1, std::min<int64_t>(kMaxChunks, ceil_div(want, tiles)));
@@ -259,6 +287,14 @@ int upload_plan(pgpu_ctx *c) {
   CK(cudaMemcpyAsync(c->d_plan, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_sysoff, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_sysn, n.data(), n.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->st));
+  std::vector<int64_t> t(2 * c->sys.size());
+  for (size_t k = 0; k < c->sys.size(); ++k) {
+    // an unrestricted system owns every slot, including particles appended later
+    const auto o = owned(c, (int)k);
+    t[2 * k] = c->sys[k].t_count < 0 ? 0 : o.first;
+    t[2 * k + 1] = c->sys[k].t_count < 0 ? INT64_MAX : o.first + o.second;
+  }
+  CK(cudaMemcpyAsync(c->d_syst, t.data(), t.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->st));
   // Pageable host sources: make sure the copies are done before the vectors go away.
   CK(cudaStreamSynchronize(c->st));
   c->plan_dirty = false;
@@ -267,9 +303,9 @@ int upload_plan(pgpu_ctx *c) {
 
 void account_pairs(pgpu_ctx *c, int launches) {
   for (size_t s = 0; s < c->sys.size(); ++s) {
-    const int64_t n = sys_n(c, (int)s);
-    c->pairs_acc += launches * n * (n > 0 ? n - 1 : 0);
-    c->selfs_acc += launches * n;
+    const int64_t n = sys_n(c, (int)s), tn = owned(c, (int)s).second;
+    c->pairs_acc += launches * tn * (n > 0 ? n - 1 : 0);
+    c->selfs_acc += launches * tn;
   }
 }
 
@@ -301,7 +337,7 @@ int launch_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
   StageArgs s;
   s.x0 = c->x0; s.acc = c->acc; s.rates = c->rates; s.sig = c->sig; s.vol = c->vol;
   s.partial = c->partial; s.P = c->P; s.Q = c->Q;
-  s.sys_off = c->d_sysoff; s.sys_n = c->d_sysn; s.nsys = (int)c->sys.size();
+  s.sys_off = c->d_sysoff; s.sys_n = c->d_sysn; s.sys_t = c->d_syst; s.nsys = (int)c->sys.size();
   s.nch = c->nch; s.cap = c->cap; s.scheme = scheme; s.stage = stage; s.dt = dt;
   for (int m = 0; m < 3; ++m) s.vinf[m] = c->cfg.vinf[m];
   s.flag = c->d_flag;
@@ -438,7 +474,8 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
-                  c->d_sysoff, c->d_sysn, c->d_plan, c->d_plan_diag, c->d_counters, c->d_nfull, c->d_flag};
+                  c->d_sysoff, c->d_sysn, c->d_syst, c->d_plan, c->d_plan_diag, c->d_counters, c->d_nfull,
+                  c->d_flag};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
@@ -577,11 +614,49 @@ int pgpu_solve(pgpu_ctx *c) {
   return collect_timing(c, 1);
 }
 
+int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t count) {
+  if (!c) return PGPU_EINVAL;
+  if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
+  if (c->sur) return fail(c, PGPU_EINVAL, "the surrogate evaluates every target of its system");
+  if (count >= 0 && first < 0) return fail(c, PGPU_EINVAL, "negative first target %lld", (long long)first);
+  SysRec &S = c->sys[system];
+  S.t_first = count < 0 ? 0 : first;
+  S.t_count = count < 0 ? -1 : count;
+  c->plan_dirty = true;
+  return PGPU_OK;
+}
+
+int pgpu_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
+  if (!c) return PGPU_EINVAL;
+  if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
+  if (stage < 0 || stage >= stages_of(scheme)) return fail(c, PGPU_EINVAL, "stage %d out of range for scheme %d", stage, scheme);
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (c->sur) return fail(c, PGPU_EINVAL, "pgpu_stage runs the direct sum only; the surrogate steps with pgpu_step");
+  int r = upload_plan(c);
+  if (r) return r;
+  if ((r = launch_eval(c, 0))) return r;
+  if ((r = launch_stage(c, scheme, stage, dt))) return r;
+  return collect_timing(c, 1);
+}
+
+int pgpu_records(pgpu_ctx *c, int32_t system, void **P, void **Q) {
+  if (!c || !P || !Q) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
+  const size_t rb = rec_bytes(c);
+  *P = static_cast<char *>(c->P) + (size_t)c->sys[system].off * rb;
+  *Q = static_cast<char *>(c->Q) + (size_t)c->sys[system].off * rb;
+  return PGPU_OK;
+}
+
 int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
   if (!c) return PGPU_EINVAL;
   if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
   if (nsteps < 0) return fail(c, PGPU_EINVAL, "negative step count");
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (restricted(c))
+    return fail(c, PGPU_EINVAL, "a context with target ranges steps stage by stage (pgpu_stage), with the source "
+                                "records of the other targets exchanged between stages");
   int r = upload_plan(c);
   if (r) return r;
   const int ns = stages_of(scheme);
@@ -622,13 +697,14 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
 int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
   if (!c || !out) return PGPU_EINVAL;
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (restricted(c)) return fail(c, PGPU_EINVAL, "diagnostics need the whole state: clear the target ranges first");
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   int r = check_contiguous(c);
   if (r) return r;
   const int shape = 2;  // 256-thread tiles for the diagnostic pair sums
   const int block = 256;
   const int nch = std::max(1, std::min(kMaxChunks, (int)ceil_div(8LL * c->sms, std::max<int64_t>(1, ceil_div(sys_n(c, system), block)))));
-  std::vector<PlanEntry> plan = build_plan(c, {system}, shape, nch);
+  std::vector<PlanEntry> plan = build_plan(c, {system}, shape, nch, false);
   CK(cudaMemcpyAsync(c->d_plan_diag, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   const bool quad = plan.size() > 1;

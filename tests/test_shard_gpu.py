@@ -1,0 +1,71 @@
+"""Target ranges and stage-by-stage stepping on one GPU: two contexts each
+own half of a ring's targets and exchange their source records between
+stages (host-ordered device copies; no kernel waits on another), and the
+result equals the unsharded graph step."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pawan_b200 import capi, cases, shard
+
+pytestmark = pytest.mark.gpu
+
+
+# FP64: the same per-target sums in the same order.  FP32C: rank 1's targets
+# start mid-tile, so warps group targets differently and a few pairs at the
+# far-regime boundary (u = 50) take the far limit on one side only; the
+# difference stays far below the 1e-5 gate.
+@pytest.mark.parametrize("prec,tol", [(capi.FP64, 1e-12), (capi.FP32C, 1e-6)])
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_two_contexts_match_unsharded_step(gpu, prec, tol, scheme):
+    w = cases.ring_gaussian(stations=10, per_section=1000, seed=2)  # 10,000 particles
+    with capi.Context(precision=prec, nu=1e-4, chunks=4) as c:
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        c.step(scheme, 0.005, 2)
+        ref_pos, ref_alpha = c.state(k)
+    bs = [shard.GpuShard(w, r, 2, precision=prec, nu=1e-4, chunks=4) for r in range(2)]
+    shard.ShardedStepper(bs, shard.LocalExchange(bs)).step(scheme, 0.005, 2)
+    pos, alpha = shard.gather_state(bs)
+    for b in bs:
+        b.close()
+    assert O.rel_err(pos - w.pos, ref_pos - w.pos) < tol
+    assert O.rel_err(alpha, ref_alpha) < tol
+
+
+def test_target_range_rules(gpu):
+    w = cases.ring_stations(stations=40)
+    with capi.Context(precision=capi.FP32C, nu=1e-4) as c:
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        c.solve()
+        v_all, a_all = c.rates(k)
+        c.set_target_range(0, 100, 300)
+        with pytest.raises(capi.PgpuError, match="stage by stage"):
+            c.step("rk4", 0.01, 1)
+        with pytest.raises(capi.PgpuError, match="whole state"):
+            c.diagnose(0)
+        with pytest.raises(capi.PgpuError):
+            c.surrogate_enable()
+        with pytest.raises(capi.PgpuError):
+            c.stage("rk4", 4, 0.01)
+        # rates of the owned targets only, equal to the full evaluation's
+        c.solve()
+        v, a = c.rates(k)
+        assert O.rel_err(v[100:400], v_all[100:400]) < 1e-6
+        assert O.rel_err(a[100:400], a_all[100:400]) < 1e-6
+        c.set_target_range(0, 0, -1)
+        c.step("rk4", 0.01, 1)
+        c.sync()
+
+
+def test_records_view_the_source_records(gpu):
+    import torch
+    w = cases.ring_stations(stations=40)
+    b = shard.GpuShard(w, 0, 1)
+    torch.cuda.synchronize()
+    P = b.P.cpu().numpy()
+    assert np.allclose(P[:, :3], w.pos, rtol=0, atol=1e-6)
+    assert np.allclose(P[:, 3], 0.5 * w.sigma ** 2, rtol=1e-6)
+    assert np.allclose(b.Q.cpu().numpy()[:, :3], w.alpha, rtol=1e-6, atol=0)
+    b.close()
