@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--surrogate-n", type=int, default=4_000_000)
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "shard"],
+                    help="N > 1: every rank its own ring (replicas, weak scaling) or one ring with its targets "
+                         "split over the ranks and the source records all-gathered per RK stage (shard, strong)")
     return ap.parse_args()
 
 
@@ -379,9 +382,124 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ one ring over N GPUs
+def run_shard(args):
+    """--mode shard: the ring's targets split over the ranks (pawan_b200.shard),
+    NCCL all-gather of the owned source records after every RK stage; value =
+    RK4 steps/s of the one ring (strong scaling)."""
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    from pawan_b200 import capi, shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29533")
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+    w = workload(args.stations)
+    n = w.n
+    b = shard.GpuShard(w, rank, world, precision=capi.FP32C, nu=NU, device=local)
+    stepper = shard.ShardedStepper(b, shard.DistExchange(b))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    shape, _ = b.ctx.autotune(reps=1)  # over this rank's owned targets (untimed)
+    for _ in range(args.warmup):
+        stepper.step("rk4", DT, 1)
+    torch.cuda.synchronize()
+    b.ctx.pair_kernel_time()
+    b.ctx.pair_counts()
+    clocks = ClockSampler(local)
+    launches0 = b.ctx.launch_count()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = 0.0
+    for i in range(args.steps):
+        if i:
+            with torch.cuda.stream(b.stream):
+                flush.zero_()
+        ev0.record(b.stream)
+        stepper.step("rk4", DT, 1)
+        ev1.record(b.stream)
+        ev1.synchronize()
+        step_ms += ev0.elapsed_time(ev1)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    launches = b.ctx.launch_count() - launches0
+    pair_ms, pair_launches = b.ctx.pair_kernel_time()
+    pairs_timed, full_timed = b.ctx.pair_counts()
+    t = torch.tensor([step_ms], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item())
+    steps_per_s = args.steps / (step_ms * 1e-3)
+
+    e2e = None
+    if not args.no_e2e:
+        # each step: the whole ring from pinned host memory, the stage-by-stage
+        # step with its exchanges, the owned rows back to the host
+        pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+        hpos, halpha, hsig, hvol = pin((n, 3)), pin((n, 3)), pin((n,)), pin((n,))
+        hpos[:], halpha[:], hsig[:], hvol[:] = w.pos, w.alpha, w.sigma, w.vol
+        from pawan_b200 import cases
+        host = cases.Wake(hpos, halpha, hsig, hvol)
+        opos, oalpha = pin((n, 3)), pin((n, 3))
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(b.stream)
+        for _ in range(args.steps):
+            b.ctx.set_particles(b.wake, host)
+            stepper.step("rk4", DT, 1)
+            b.ctx.state(b.wake, out=(opos, oalpha))
+        e1.record(b.stream)
+        e1.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": args.steps / (float(te.item()) * 1e-3), "unit": "steps/s",
+               "h2d_bytes_per_step": int(hpos.nbytes + halpha.nbytes + hsig.nbytes + hvol.nbytes),
+               "d2h_bytes_per_step": int(opos.nbytes + oalpha.nbytes)}
+
+    if rank == 0:
+        ffma_peak, ffma2_peak = capi.fp32_peaks(local)
+        fp32_peak = max(ffma_peak, ffma2_peak)
+        pair_avg_ms = pair_ms / max(pair_launches, 1)
+        flops_per_launch = (FLOPS_PER_PAIR * full_timed + FLOPS_PER_FAR_PAIR * (pairs_timed - full_timed)) / max(pair_launches, 1)
+        achieved = flops_per_launch / (pair_avg_ms * 1e-3) / 1e12
+        out = {
+            "metric": "RK4 steps/s", "value": steps_per_s, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": n, "parallelism": f"targets{world}",
+                       "pair_kernel_shape": {"block": shape[0], "targets_per_thread": shape[1]},
+                       "exchange": f"NCCL all-gather of the FP32 source records after each RK stage ({32 * n} B)",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "precision": "FP32 pairs, compensated sums, FP64 state"},
+            "pair_interactions_per_s": 4 * n * (n - 1) * steps_per_s,
+            "pair_kernel_ms": pair_avg_ms,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": None,
+                         "note": "rank 0's pair kernel over its owned targets; peak as in the replicas mode"},
+            "cpu_baseline": None,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(out))
+    b.close()
+    dist.destroy_process_group()
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.mode == "shard":
+        run_shard(a)
     else:
         run_ours(a)
