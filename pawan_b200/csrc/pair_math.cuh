@@ -238,6 +238,41 @@ __device__ __forceinline__ PairTerms<float> pair_terms_near(float r2, float s2) 
   return o;
 }
 
+// Two pairs at once (lanes .x and .y of every float2, packed FP32 of sm_100):
+// the mid branch of pair_terms_near, valid for u = r2 / s2 >= 1.  For
+// u >= 50 its e^{-u/2} terms fall below 1.4e-11 and it equals the far limit
+// to FP32 rounding.  Lanes with u < 1 (the self pair among them) must be
+// redone with pair_terms_near.  -P and -B are formed with negated
+// coefficients, so each lane rounds exactly as the scalar branch does.
+struct PairTerms2 {
+  float2 q, F, zd;
+};
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ PairTerms2 pair_terms_mid2(float2 r2, float2 s2) {
+  const float2 is = make_float2(fast_rsqrt(s2.x), fast_rsqrt(s2.y));
+  const float2 is2 = __fmul2_rn(is, is);
+  const float2 ea = __fmul2_rn(__fmul2_rn(r2, is2), dup2((float)kNegHalfLog2e));
+  const float2 E = make_float2(fast_exp2(ea.x), fast_exp2(ea.y));
+  const float2 z = __fmul2_rn(__fmul2_rn(__fmul2_rn(dup2((float)kK1), is), is2), E);  // (k1 s) s^2 E
+  const float2 ir = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
+  const float2 A = __fmul2_rn(ir, ir);
+  const float2 zs = __fmul2_rn(__fmul2_rn(dup2(1.41421356237309515f), s2), is);  // sqrt2 sigma
+  const float2 t = __ffma2_rn(__fmul2_rn(dup2(kErfcxA), zs), ir, dup2(kErfcxB));
+  float2 np = dup2(-PGPU_E10);
+  np = __ffma2_rn(np, t, dup2(-PGPU_E9)); np = __ffma2_rn(np, t, dup2(-PGPU_E8));
+  np = __ffma2_rn(np, t, dup2(-PGPU_E7)); np = __ffma2_rn(np, t, dup2(-PGPU_E6));
+  np = __ffma2_rn(np, t, dup2(-PGPU_E5)); np = __ffma2_rn(np, t, dup2(-PGPU_E4));
+  np = __ffma2_rn(np, t, dup2(-PGPU_E3)); np = __ffma2_rn(np, t, dup2(-PGPU_E2));
+  np = __ffma2_rn(np, t, dup2(-PGPU_E1)); np = __ffma2_rn(np, t, dup2(-PGPU_E0));
+  const float2 nB = __ffma2_rn(__fmul2_rn(zs, A), np, __fmul2_rn(dup2(-(float)kK1), is));
+  PairTerms2 o;
+  o.q = __ffma2_rn(__fmul2_rn(E, A), nB, __fmul2_rn(A, ir));
+  o.F = __fmul2_rn(__ffma2_rn(dup2(-3.0f), o.q, z), A);
+  o.zd = __fmul2_rn(z, is2);
+  return o;
+}
+
 // Error-free addition (Knuth two-sum): hi + lo == a + b exactly.  The
 // explicit _rn intrinsics keep the compiler from contracting or reordering.
 __device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float b) {

@@ -247,73 +247,7 @@ struct TreeEvalArgs {
 };
 
 constexpr int kTreeBlock = 256;  // sampled-check kernel
-constexpr int kLeafBlock = 512;  // one thread per target of a leaf (leaves hold <= 512)
-constexpr int kFarChunk = 32;
 
-// One CTA per target leaf, one thread per target.  Warps past the end of the
-// leaf only help stage shared memory; they issue no arithmetic.
-__global__ void __launch_bounds__(kLeafBlock) tree_eval_kernel(TreeEvalArgs a) {
-  __shared__ float sc[kFarChunk][kCellFloats];
-  __shared__ float4 sP[kLeafBlock], sQ[kLeafBlock];
-  const int tid = threadIdx.x;
-  for (int li = blockIdx.x; li < a.nleaves; li += gridDim.x) {
-    const TreeCell tc = a.cells[a.leaves[li]];
-    const bool active = tc.start + (tid & ~31) < tc.end;  // warp-uniform
-    const int t = min(tc.start + tid, tc.end - 1);
-    const float4 pt = a.Ps[t], qt = a.Qs[t];
-    const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
-    const float hst = pt.w, h50 = kFarU * pt.w, vt = qt.w;
-    float vh[3] = {0, 0, 0}, vl[3] = {0, 0, 0}, dh[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
-    // ---- far cells, in chunks staged in shared memory
-    const int fo = a.far_off[li], fn = a.far_cnt[li];
-    for (int c0 = 0; c0 < fn; c0 += kFarChunk) {
-      const int cn = min(kFarChunk, fn - c0);
-      __syncthreads();
-      for (int e = tid; e < cn * kCellFloats; e += kLeafBlock)
-        sc[e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
-      __syncthreads();
-      if (active) {
-        float su[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
-        for (int j = 0; j < cn; ++j) {
-          float u[3], s[3];
-          far_expand(sc[j], xt, at, a.order, u, s);
-          for (int m = 0; m < 3; ++m) { su[m] += u[m]; ss[m] += s[m]; }
-        }
-        for (int m = 0; m < 3; ++m) {
-          two_sum_acc(vh[m], vl[m], su[m]);
-          two_sum_acc(dh[m], dl[m], ss[m]);
-        }
-      }
-    }
-    // ---- near field, exact, over sorted-order runs in tiles of kLeafBlock records
-    const int no = a.near_off[li], nn = a.near_cnt[li];
-    for (int ni = 0; ni < nn; ++ni) {
-      const int2 run = a.near_runs[no + ni];
-      for (int sb = run.x; sb < run.y; sb += kLeafBlock) {
-        __syncthreads();
-        const int j = sb + tid;
-        if (j < run.y) { sP[tid] = a.Ps[j]; sQ[tid] = a.Qs[j]; }
-        __syncthreads();
-        if (active) {
-          const int cnt = min(kLeafBlock, run.y - sb);
-          for (int g = 0; g < cnt; g += 32) {
-            float sv[3] = {}, sd[3] = {}, sp[3] = {}, sdv[3] = {};
-            const int gn = min(32, cnt - g);
-            for (int jj = 0; jj < gn; ++jj) pair_accum_f32(sP[g + jj], sQ[g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
-            fold_group(at, a.nu2, sv, sd, sp, sdv, vh, vl, dh, dl);
-          }
-        }
-      }
-    }
-    if (tc.start + tid < tc.end) {
-      double *o = a.partial + a.off + a.idx[tc.start + tid];
-      for (int m = 0; m < 3; ++m) {
-        o[m * a.cap] = ((double)vh[m] + (double)vl[m]) * kInv4Pi;
-        o[(3 + m) * a.cap] = ((double)dh[m] + (double)dl[m]) * kInv4Pi;
-      }
-    }
-  }
-}
 
 // Warp-independent form: every warp takes work items (target leaf, slice of
 // 32 of its targets) from an atomic counter and stages its own source tiles,
@@ -404,6 +338,15 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
         two_sum_acc(dh[m], dl[m], ss[m]);
       }
     }
+    // Near field: nearly every pair here is inside u < 50, so every pair takes
+    // the closed form, two sources per packed FP32 instruction (lane .x the
+    // even source of a pair, .y the odd one; pair-interleaved staging as in
+    // the direct kernel); lanes at u < 1, the self pair among them, take the
+    // series.
+    const float2 X2[3] = {dup2(xt[0]), dup2(xt[1]), dup2(xt[2])};
+    const float2 AT2[3] = {dup2(at[0]), dup2(at[1]), dup2(at[2])};
+    const float2 NAT2[3] = {dup2(-at[0]), dup2(-at[1]), dup2(-at[2])};
+    const float2 HS2 = dup2(hst), VT2 = dup2(vt), M1 = dup2(-1.f);
     const int no = a.near_off[li], nn = a.near_cnt[li];
     for (int ni = 0; ni < nn; ++ni) {
       const int2 run = a.near_runs[no + ni];
@@ -411,15 +354,67 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
         __syncwarp();
         for (int k = lane; k < kWarpTile; k += 32) {
           const int j = sb + k;
-          if (j < run.y) { ws.sP[k] = a.Ps[j]; ws.sQ[k] = a.Qs[j]; }
+          const float4 p = j < run.y ? a.Ps[j] : pad_P<float>();
+          const float4 q = j < run.y ? a.Qs[j] : pad_Q<float>();
+          float *dp = reinterpret_cast<float *>(ws.sP) + (k >> 1) * 8 + (k & 1);
+          float *dq = reinterpret_cast<float *>(ws.sQ) + (k >> 1) * 8 + (k & 1);
+          dp[0] = p.x; dp[2] = p.y; dp[4] = p.z; dp[6] = p.w;
+          dq[0] = q.x; dq[2] = q.y; dq[4] = q.z; dq[6] = q.w;
         }
         __syncwarp();
-        const int cnt = min(kWarpTile, run.y - sb);
-        for (int g = 0; g < cnt; g += 32) {
-          float sv[3] = {}, sd[3] = {}, sp[3] = {}, sdv[3] = {};
-          const int gn = min(32, cnt - g);
-          for (int jj = 0; jj < gn; ++jj)
-            pair_accum_f32(ws.sP[g + jj], ws.sQ[g + jj], xt, at, hst, h50, vt, sv, sd, sp, sdv);
+        // source pairs; an odd tail pairs with a padding source (zero strength, far away)
+        const int npr = (min(kWarpTile, run.y - sb) + 1) >> 1;
+        for (int g = 0; g < npr; g += 16) {
+          float2 sv2[3], sd2[3], sp2[3], sdv2[3];
+          for (int m = 0; m < 3; ++m) { sv2[m] = sd2[m] = sp2[m] = sdv2[m] = dup2(0.f); }
+          const int ge = min(npr, g + 16);
+          for (int r = g; r < ge; ++r) {
+            const float4 pa = ws.sP[2 * r], pb = ws.sP[2 * r + 1];
+            const float4 qa = ws.sQ[2 * r], qb = ws.sQ[2 * r + 1];
+            const float2 dx = __ffma2_rn(make_float2(pa.x, pa.y), M1, X2[0]);
+            const float2 dy = __ffma2_rn(make_float2(pa.z, pa.w), M1, X2[1]);
+            const float2 dz = __ffma2_rn(make_float2(pb.x, pb.y), M1, X2[2]);
+            const float2 ax = make_float2(qa.x, qa.y), ay = make_float2(qa.z, qa.w), az = make_float2(qb.x, qb.y);
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            const float2 s2 = __fadd2_rn(HS2, make_float2(pb.z, pb.w));
+            PairTerms2 t = pair_terms_mid2(r2, s2);
+            const bool lx = r2.x < s2.x, ly = r2.y < s2.y;  // u < 1
+            if (__any_sync(0xffffffffu, lx || ly)) {
+              if (lx) { const PairTerms<float> e = pair_terms_near(r2.x, s2.x); t.q.x = e.q; t.F.x = e.F; t.zd.x = e.zd; }
+              if (ly) { const PairTerms<float> e = pair_terms_near(r2.y, s2.y); t.q.y = e.q; t.F.y = e.F; t.zd.y = e.zd; }
+            }
+            // w = alpha_s x d (scalar: the negated operand is free)
+            const float2 wx = make_float2(ay.x * dz.x - az.x * dy.x, ay.y * dz.y - az.y * dy.y);
+            const float2 wy = make_float2(az.x * dx.x - ax.x * dz.x, az.y * dx.y - ax.y * dz.y);
+            const float2 wz = make_float2(ax.x * dy.x - ay.x * dx.x, ax.y * dy.y - ay.y * dx.y);
+            sv2[0] = __ffma2_rn(t.q, wx, sv2[0]);
+            sv2[1] = __ffma2_rn(t.q, wy, sv2[1]);
+            sv2[2] = __ffma2_rn(t.q, wz, sv2[2]);
+            float2 dot = __fmul2_rn(AT2[0], wx);
+            dot = __ffma2_rn(AT2[1], wy, dot);
+            dot = __ffma2_rn(AT2[2], wz, dot);
+            const float2 fd = __fmul2_rn(t.F, dot);
+            sd2[0] = __ffma2_rn(fd, dx, sd2[0]);
+            sd2[1] = __ffma2_rn(fd, dy, sd2[1]);
+            sd2[2] = __ffma2_rn(fd, dz, sd2[2]);
+            sp2[0] = __ffma2_rn(t.q, ax, sp2[0]);
+            sp2[1] = __ffma2_rn(t.q, ay, sp2[1]);
+            sp2[2] = __ffma2_rn(t.q, az, sp2[2]);
+            // diffusion per pair: zeta (v_t a_s - v_s a_t), as in DIFFUSION (interaction_utils.h:358-369)
+            const float2 vs = make_float2(qb.z, qb.w);
+            sdv2[0] = __ffma2_rn(t.zd, __ffma2_rn(vs, NAT2[0], __fmul2_rn(VT2, ax)), sdv2[0]);
+            sdv2[1] = __ffma2_rn(t.zd, __ffma2_rn(vs, NAT2[1], __fmul2_rn(VT2, ay)), sdv2[1]);
+            sdv2[2] = __ffma2_rn(t.zd, __ffma2_rn(vs, NAT2[2], __fmul2_rn(VT2, az)), sdv2[2]);
+          }
+          float sv[3], sd[3], sp[3], sdv[3];
+          for (int m = 0; m < 3; ++m) {
+            sv[m] = sv2[m].x + sv2[m].y;
+            sd[m] = sd2[m].x + sd2[m].y;
+            sp[m] = sp2[m].x + sp2[m].y;
+            sdv[m] = sdv2[m].x + sdv2[m].y;
+          }
           fold_group(at, a.nu2, sv, sd, sp, sdv, vh, vl, dh, dl);
         }
       }
