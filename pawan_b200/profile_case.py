@@ -51,8 +51,11 @@ def main() -> None:
     if a.steps:
         c.step("rk4", 0.005, a.steps)
         c.sync()
+    import time
+    c.sync()
+    t = time.perf_counter()
     d, vbi = c.diagnose(0)
-    print("diagnostics", d.tolist(), "vbi", vbi.tolist())
+    print(f"diagnose {1e3 * (time.perf_counter() - t):.1f} ms; diagnostics", d.tolist(), "vbi", vbi.tolist())
     c.close()
 
 
