@@ -560,7 +560,12 @@ template <typename T> struct DiagArgs {
 //   helicity  q(rho, s_ts) (x_s - x_t).(a_t x a_s)            (HELICITY, interaction_utils.h:214-242)
 //   KE        [(rho^2 + 2 s^2) a_t.a_s + (d.a_t)(d.a_s)] / (16 pi (rho^2 + s^2)^1.5)   (:278-306)
 //   KEF       (rho^2 + 1.5 s^2) a_t.a_s / (8 pi (rho^2 + s^2)^1.5)                    (:308-331)
-// Summed over ordered pairs these equal PAWAN's 2 x sum over unordered pairs.
+// All three terms are symmetric in (t, s), so each unordered pair is
+// evaluated once, from its lower index (sources s > t only), and the row sums
+// are doubled: they then equal sums over ordered pairs, PAWAN's 2 x sum over
+// unordered pairs.  In FP32 the helicity's q takes the far limit 1/rho^3 for
+// u >= 50 (as in the rate kernel) and the mid/series terms only when some lane
+// of the warp needs them.
 template <typename T, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
   __shared__ __align__(16) v4_t<T> sP[BLOCK];
@@ -576,11 +581,15 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
     const int64_t tile = local / a.nch;
     const int c = (int)(local - tile * a.nch);
     const int64_t tend = pe.off + pe.n;
-    const int64_t t = min(pe.off + tile * BLOCK + tid, tend - 1);
-    const bool valid = pe.off + tile * BLOCK + tid < tend;
-    const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
-    const int64_t s1 = min(s0 + pe.chunk, tend);
+    const int64_t tlo = pe.off + tile * BLOCK;  // first target of the tile
+    const int64_t t = min(tlo + tid, tend - 1);
+    const bool valid = tlo + tid < tend;
+    // sources above the tile's first target only (s > t is tested per pair
+    // while a tile can still hold s <= t)
+    const int64_t s0 = max(pe.off + (int64_t)c * pe.chunk, tlo);
+    const int64_t s1 = min(pe.off + (int64_t)c * pe.chunk + pe.chunk, tend);
     const v4_t<T> pt = a.P[t], qt = a.Q[t];
+    const T h50 = T(kFarU) * pt.w;
     double h = 0, ke = 0, kef = 0;
     for (int64_t sb = s0; sb < s1; sb += BLOCK) {
       __syncthreads();
@@ -590,15 +599,25 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
       __syncthreads();
       T hh = 0, kk = 0, kf = 0;
       const int cnt = (int)min((int64_t)BLOCK, s1 - sb);
+      const bool diag = sb <= tlo + BLOCK - 1;  // the tile may still see s <= t
       for (int jj = 0; jj < cnt; ++jj) {
-        if (sb + jj == t) continue;
+        const bool use = !diag || sb + jj > t;
         const v4_t<T> p = sP[jj], q = sQ[jj];
         const T dx = pt.x - p.x, dy = pt.y - p.y, dz = pt.z - p.z;
         const T r2 = dx * dx + dy * dy + dz * dz;
         const T s2 = pt.w + p.w;
-        const PairTerms<T> k = pair_terms(r2, s2);
+        T kq;
+        if constexpr (sizeof(T) == 4) {
+          const bool near = fmaf(-kFarU, p.w, r2) < h50;
+          const float ir = fast_rsqrt(r2);
+          kq = ir * ir * ir;
+          if (__any_sync(0xffffffffu, near && use)) {
+            if (near && use) kq = pair_terms_near(r2, s2).q;
+          }
+        } else {
+          kq = pair_terms(r2, s2).q;
+        }
         const T cx = qt.y * q.z - qt.z * q.y, cy = qt.z * q.x - qt.x * q.z, cz = qt.x * q.y - qt.y * q.x;
-        hh -= k.q * (dx * cx + dy * cy + dz * cz);
         const T aa = qt.x * q.x + qt.y * q.y + qt.z * q.z;
         const T dat = dx * qt.x + dy * qt.y + dz * qt.z;
         const T das = dx * q.x + dy * q.y + dz * q.z;
@@ -606,18 +625,22 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
         T ir;
         if constexpr (sizeof(T) == 4) ir = fast_rsqrt(rs); else ir = rsqrt(rs);
         const T ir3 = ir * ir * ir;
-        kk += ((r2 + T(2) * s2) * aa + dat * das) * ir3;
-        kf += (r2 + T(1.5) * s2) * aa * ir3;
+        if (use) {
+          hh -= kq * (dx * cx + dy * cy + dz * cz);
+          kk += ((r2 + T(2) * s2) * aa + dat * das) * ir3;
+          kf += (r2 + T(1.5) * s2) * aa * ir3;
+        }
       }
       h += (double)hh;
       ke += (double)kk;
       kef += (double)kf;
     }
     if (valid) {
+      // doubled: each unordered pair was summed once
       double *o = a.partial + (int64_t)c * 6 * a.cap + t;
-      o[0] = h * kInv4Pi;
-      o[a.cap] = ke * (kInv4Pi * 0.25);      // 1/(16 pi)
-      o[2 * a.cap] = kef * (kInv4Pi * 0.5);  // 1/(8 pi)
+      o[0] = h * (2.0 * kInv4Pi);
+      o[a.cap] = ke * (2.0 * kInv4Pi * 0.25);      // 1/(16 pi)
+      o[2 * a.cap] = kef * (2.0 * kInv4Pi * 0.5);  // 1/(8 pi)
     }
   }
 }
