@@ -55,6 +55,7 @@ N_STATIONS, N_SECTION = 1000, 1000
 SIGMA, NU, DT = 0.02, 1e-4, 0.005
 FLOPS_PER_PAIR = 95  # algorithmic count of one ordered pair interaction (full formula)
 FLOPS_PER_FAR_PAIR = 59  # same tally with erf = 1 and exp(-u/2) = 0 (far-field limit, u >= 50)
+DIAG_FLOPS_PER_PAIR = 85  # helicity + KE + KEF per unordered pair (algorithmic count)
 SAMPLE_N = 4000      # particles in the bounded CPU sample
 WORKLOAD = "vortex ring N=1M (1000 stations x 1000/section, gaussian core a=0.1, sigma=0.02), RK4 dt=0.005, FP32c pairs + FP64 state"
 
@@ -326,6 +327,24 @@ def run_ours(args):
                "d2h_bytes_per_step": int(opos.nbytes + oalpha.nbytes),
                "wall_s": time.perf_counter() - t0}
 
+    # conserved-quantity diagnostics (pgpu_diagnose) of the same ring, outside
+    # the timed region: one warm call, then one timed with CUDA events
+    diag = None
+    if rank == 0:
+        ctx.diagnose(0)
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        d0.record(stream)
+        ctx.diagnose(0)
+        d1.record(stream)
+        d1.synchronize()
+        dms = d0.elapsed_time(d1)
+        dflops = DIAG_FLOPS_PER_PAIR * n * (n - 1) / 2
+        diag = {"ms": dms, "unordered_pairs": n * (n - 1) // 2,
+                "achieved_tflops": dflops / (dms * 1e-3) / 1e12,
+                "note": f"{DIAG_FLOPS_PER_PAIR} flop per unordered pair (helicity 42 + KE 25 + KEF 18); "
+                        "frac against the same FP32 peak as the step's roofline"}
+
     sur = None
     if rank == 0 and not args.no_surrogate:
         ctx.close()
@@ -345,6 +364,8 @@ def run_ours(args):
             for m in re.finditer(r"traffic_bytes_per_launch\[N=(\d+)[^\]]*\]\s*=\s*(\d+)", tf.read_text()):
                 if int(m.group(1)) == n:
                     traffic = int(m.group(2))
+        if diag is not None:
+            diag["frac"] = diag["achieved_tflops"] / fp32_peak
         cpu = None
         from oracle import oracle as O
         if O.ref_available():
@@ -373,6 +394,7 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "diagnostics": diag,
             "surrogate": sur,
         }
         print(json.dumps(out))
