@@ -150,6 +150,15 @@ int pgpu_probe(pgpu_ctx *ctx, int32_t system, int64_t npts, const double *pts, d
 /* Waits for all queued work; reports PGPU_ENUMERIC if a step produced a
  * non-finite state. */
 int pgpu_sync(pgpu_ctx *ctx);
+/* Pair-kernel timing (pgpu_pair_kernel_time) is on by default.  Reading the
+ * CUDA-event times makes pgpu_solve / pgpu_step / pgpu_stage wait for their
+ * pair kernels; with timing off (on = 0) those calls only queue work, and
+ * pgpu_sync or pgpu_sync_timeout waits.  No PAWAN counterpart. */
+int pgpu_set_timing(pgpu_ctx *ctx, int on);
+/* pgpu_sync with a host watchdog: returns PGPU_ETIMEOUT if the queued work has
+ * not finished after `seconds` (the work is left running; a later pgpu_sync
+ * waits for it), else as pgpu_sync.  No PAWAN counterpart. */
+int pgpu_sync_timeout(pgpu_ctx *ctx, double seconds);
 
 /* Device time in milliseconds of the pair kernel launches since the last call
  * (CUDA events on the context stream), and the number of them. */

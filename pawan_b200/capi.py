@@ -38,6 +38,7 @@ EXPORTS = [
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
     "pgpu_rates_noalloc", "pgpu_noalloc_last_error", "pgpu_set_target_range", "pgpu_stage", "pgpu_records",
+    "pgpu_sync_timeout", "pgpu_set_timing",
 ]
 
 
@@ -145,6 +146,8 @@ def load(build_if_missing: bool = False):
         "pgpu_set_target_range": (C.c_int, [vp, C.c_int32, C.c_int64, C.c_int64]),
         "pgpu_stage": (C.c_int, [vp, C.c_int, C.c_int, C.c_double]),
         "pgpu_records": (C.c_int, [vp, C.c_int32, C.POINTER(vp), C.POINTER(vp)]),
+        "pgpu_sync_timeout": (C.c_int, [vp, C.c_double]),
+        "pgpu_set_timing": (C.c_int, [vp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -292,8 +295,17 @@ class Context:
         s = SCHEMES[scheme] if isinstance(scheme, str) else scheme
         self._ck(self.lib.pgpu_step(self.h, s, float(dt), int(nsteps)))
 
-    def sync(self):
-        self._ck(self.lib.pgpu_sync(self.h))
+    def set_timing(self, on: bool):
+        """Pair-kernel timing on (default; calls wait for their pair kernels) or off (calls only queue work)."""
+        self._ck(self.lib.pgpu_set_timing(self.h, 1 if on else 0))
+
+    def sync(self, timeout: float | None = None):
+        """Waits for the queued work; with `timeout` (seconds) a host watchdog
+        raises PgpuError(PGPU_ETIMEOUT) instead of waiting longer."""
+        if timeout is None:
+            self._ck(self.lib.pgpu_sync(self.h))
+        else:
+            self._ck(self.lib.pgpu_sync_timeout(self.h, float(timeout)))
 
     def diagnose(self, system: int = 0):
         out = np.zeros(15)

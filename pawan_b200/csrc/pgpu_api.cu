@@ -15,10 +15,14 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <map>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -95,13 +99,20 @@ struct pgpu_ctx {
   double pair_ms = 0.0;
   int64_t pair_launches = 0;
   int64_t launches = 0;
-  std::map<std::tuple<int, double, int, int>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int, double, int, int, bool>, cudaGraphExec_t> graphs;  // (scheme, dt, shape, nch, timing)
   std::vector<cudaGraph_t> graph_defs;
   std::string err;
   SurrogateState *sur = nullptr;  // far-field surrogate of the single system, when enabled
 };
 
 namespace {
+
+// NVTX range over an entry point (header-only NVTX3: a no-op unless a
+// profiler is attached), so profiler timelines show the library's phases.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
   char buf[512];
@@ -113,10 +124,16 @@ int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
   return code;
 }
 
+// On failure the per-thread last error is reset (cudaGetLastError), so a
+// non-sticky error such as a failed allocation is reported once, by the call
+// that met it, and not again by the next healthy launch.
 #define CK(call)                                                                                    \
   do {                                                                                              \
     cudaError_t e_ = (call);                                                                        \
-    if (e_ != cudaSuccess) return fail(c, PGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    if (e_ != cudaSuccess) {                                                                        \
+      cudaGetLastError();                                                                           \
+      return fail(c, PGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_));                   \
+    }                                                                                               \
   } while (0)
 
 bool fp64(const pgpu_ctx *c) { return c->cfg.precision == PGPU_FP64; }
@@ -167,7 +184,10 @@ int freeze(pgpu_ctx *c) {
   const int64_t cap = c->cap;
   auto alloc = [&](void **p, size_t bytes) -> int {
     cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) return fail(c, PGPU_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      cudaGetLastError();  // a failed allocation must not surface again at the next launch
+      return fail(c, PGPU_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
     return PGPU_OK;
   };
   int r;
@@ -605,6 +625,7 @@ int pgpu_get_rates_flat(pgpu_ctx *c, double *rate, const int64_t *maxn, int32_t 
 }
 
 int pgpu_solve(pgpu_ctx *c) {
+  NvtxRange nvtx("pgpu_solve");
   if (!c) return PGPU_EINVAL;
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   int r = upload_plan(c);
@@ -627,6 +648,7 @@ int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t co
 }
 
 int pgpu_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
+  NvtxRange nvtx("pgpu_stage");
   if (!c) return PGPU_EINVAL;
   if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
   if (stage < 0 || stage >= stages_of(scheme)) return fail(c, PGPU_EINVAL, "stage %d out of range for scheme %d", stage, scheme);
@@ -650,6 +672,7 @@ int pgpu_records(pgpu_ctx *c, int32_t system, void **P, void **Q) {
 }
 
 int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
+  NvtxRange nvtx("pgpu_step");
   if (!c) return PGPU_EINVAL;
   if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
   if (nsteps < 0) return fail(c, PGPU_EINVAL, "negative step count");
@@ -667,7 +690,7 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
     }
     return PGPU_OK;
   }
-  auto key = std::make_tuple(scheme, dt, c->shape, c->nch);
+  auto key = std::make_tuple(scheme, dt, c->shape, c->nch, c->timing);
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
@@ -695,6 +718,7 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
 }
 
 int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
+  NvtxRange nvtx("pgpu_diagnose");
   if (!c || !out) return PGPU_EINVAL;
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (restricted(c)) return fail(c, PGPU_EINVAL, "diagnostics need the whole state: clear the target ranges first");
@@ -793,6 +817,28 @@ int pgpu_sync(pgpu_ctx *c) {
     }
   }
   return PGPU_OK;
+}
+
+int pgpu_set_timing(pgpu_ctx *c, int on) {
+  if (!c) return PGPU_EINVAL;
+  c->timing = on != 0;
+  return PGPU_OK;
+}
+
+int pgpu_sync_timeout(pgpu_ctx *c, double seconds) {
+  if (!c) return PGPU_EINVAL;
+  NvtxRange nvtx("pgpu_sync_timeout");
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaStreamQuery(c->st);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) return fail(c, PGPU_ECUDA, "cudaStreamQuery failed: %s", cudaGetErrorString(e));
+    const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (waited > seconds)
+      return fail(c, PGPU_ETIMEOUT, "the queued work did not finish within %.3f s (it keeps running)", seconds);
+    std::this_thread::sleep_for(std::chrono::microseconds(100));
+  }
+  return pgpu_sync(c);
 }
 
 int pgpu_pair_kernel_time(pgpu_ctx *c, double *ms, int64_t *launches) {

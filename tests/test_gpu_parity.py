@@ -358,3 +358,41 @@ def test_conservation_and_fp32c_trajectory(gpu):
     assert last["fp32c"]["total vorticity"] < 1e-9
     assert last["fp32c_vs_fp64"]["displacement"] < TOL[capi.FP32C]
     assert last["fp32c_vs_fp64"]["alpha"] < TOL[capi.FP32C]
+
+
+def test_watchdog_times_out_and_work_completes(gpu):
+    """Host-side failure detection: a sync with a short deadline on a queued
+    RK4 step of a 400k ring returns PGPU_ETIMEOUT without disturbing the work;
+    the next plain sync waits for it and the context stays usable."""
+    w = cases.ring_gaussian(stations=400, per_section=1000, seed=1)
+    with capi.Context(precision=capi.FP32C, nu=1e-4) as c:
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        c.set_timing(False)  # the step only queues its work
+        c.step("rk4", 0.005, 1)
+        with pytest.raises(capi.PgpuError) as e:
+            c.sync(timeout=0.01)
+        assert e.value.code == capi.PGPU_ETIMEOUT
+        c.sync()
+        c.sync(timeout=60.0)
+        pos, _ = c.state(k)
+        assert np.all(np.isfinite(pos))
+
+
+def test_device_allocation_failure_is_reported(gpu):
+    """A context whose capacity cannot be allocated (2^31 - 1 particles, about
+    2 TB) fails with PGPU_ENOMEM at the first upload, frees what it got, and
+    a normal context works afterwards."""
+    w = cases.ring_stations(stations=40)
+    c = capi.Context(precision=capi.FP32C, nu=1e-4)
+    k = c.add_wake(2 ** 31 - 1)
+    with pytest.raises(capi.PgpuError) as e:
+        c.set_particles(k, w)
+    assert e.value.code == capi.PGPU_ENOMEM
+    c.close()
+    with capi.Context(precision=capi.FP32C, nu=1e-4) as c2:
+        k2 = c2.add_wake(w.n)
+        c2.set_particles(k2, w)
+        c2.solve()
+        v, _ = c2.rates(k2)
+        assert np.all(np.isfinite(v))
