@@ -34,6 +34,10 @@ constexpr int kMaxChunks = 16;
 // sums over this many sources, then one error-free two-sum per component.
 constexpr int kPairCG = 64;
 constexpr int kDiagFields = 19;
+// FP64 far regime: u = rho^2 / sigma^2 >= 100, where erfc(sqrt(u/2)) and the
+// e^{-u/2} terms of q and F vanish at double precision (the closed form and
+// the far limit agree to the last bit from u ~ 90 on).
+constexpr double kFarU64 = 100.0;
 
 // One system in the work list (sorted by decreasing work).
 struct PlanEntry {
@@ -329,11 +333,24 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
                 }
               }
             } else {
-              const PairTerms<T> pt = pair_terms(r2, hst[k] + p.w);
-              qq = pt.q; FF = pt.F;
-              sdv[k][0] += pt.zd * (vt[k] * q.x - q.w * at[k][0]);
-              sdv[k][1] += pt.zd * (vt[k] * q.y - q.w * at[k][1]);
-              sdv[k][2] += pt.zd * (vt[k] * q.z - q.w * at[k][2]);
+              // FP64: for u >= kFarU64 the far limit equals the closed form to
+              // double rounding (erfc(sqrt(u/2)) and the e^{-u/2} terms are
+              // below 1e-16 of q and F); the closed form runs under a vote
+              const T s2 = hst[k] + p.w;
+              const bool near = r2 < T(kFarU64) * s2;
+              const T ir = rsqrt(r2);
+              const T A = ir * ir;
+              qq = A * ir;
+              FF = T(-3) * qq * A;
+              if (__any_sync(0xffffffffu, near)) {
+                if (near) {
+                  const PairTerms<T> pt = pair_terms(r2, s2);
+                  qq = pt.q; FF = pt.F;
+                  sdv[k][0] += pt.zd * (vt[k] * q.x - q.w * at[k][0]);
+                  sdv[k][1] += pt.zd * (vt[k] * q.y - q.w * at[k][1]);
+                  sdv[k][2] += pt.zd * (vt[k] * q.z - q.w * at[k][2]);
+                }
+              }
             }
             // w = alpha_s x d
             const T wx = q.y * dz - q.z * dy;
@@ -615,7 +632,12 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
             if (near && use) kq = pair_terms_near(r2, s2).q;
           }
         } else {
-          kq = pair_terms(r2, s2).q;
+          const bool near = r2 < T(kFarU64) * s2;
+          const T ir = rsqrt(r2);
+          kq = ir * ir * ir;
+          if (__any_sync(0xffffffffu, near && use)) {
+            if (near && use) kq = pair_terms(r2, s2).q;
+          }
         }
         const T cx = qt.y * q.z - qt.z * q.y, cy = qt.z * q.x - qt.x * q.z, cz = qt.x * q.y - qt.y * q.x;
         const T aa = qt.x * q.x + qt.y * q.y + qt.z * q.z;

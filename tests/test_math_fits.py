@@ -70,3 +70,21 @@ def test_far_limit_error_bound():
         assert abs(1 / x ** 3 - q) < 1e-9 * q
         assert abs(-3 / x ** 5 - F) < 2e-9 * abs(F)
         assert math.exp(-u / 2) < 1.4e-11
+
+
+def test_fp64_far_limit_is_exact_to_double_rounding():
+    """FP64 kernels take q' = r^-3, F' = -3 r^-5 for u = rho^2 / sigma^2 >= 100:
+    the closed form (gaussian.h:47-60) equals that limit to a few units of
+    double rounding there (the erfc and e^{-u/2} terms are below 1e-21 of
+    them; what remains is the rounding of the two ways of evaluating)."""
+    import math
+    for u in np.linspace(100.0, 400.0, 200):
+        rb = math.sqrt(u)  # rho / sigma, sigma = 1
+        zeta = math.exp(-0.5 * u) / (2 * math.pi) ** 1.5
+        phi = math.erf(rb / math.sqrt(2)) / (4 * math.pi)
+        q = (phi / rb - zeta) / rb ** 2
+        F = (zeta - 3 * q) / rb ** 2
+        q_far = 1 / (4 * math.pi * rb ** 3)
+        F_far = -3 * q_far / rb ** 2
+        assert abs(q - q_far) <= 1e-15 * q_far
+        assert abs(F - F_far) <= 1e-15 * abs(F_far)
