@@ -17,7 +17,11 @@
 //   (ax0, ax1, ay0, ay1), (az0, az1, vol0, vol1).  Each source is copied with
 //   four 4-byte cp.async per record, so one 16-byte shared load yields two
 //   float2 operands.
-// * Cross products stay scalar, where a negated operand is free.
+// * In all-far tiles, positions are taken relative to the tile's first
+//   source, which turns the per-pair cross product alpha_s x d into per-source
+//   and per-group work (see the far loop): 25 packed FP32 operations per far
+//   pair.  In the other tiles cross products stay scalar, where a negated
+//   operand is free.
 #pragma once
 
 namespace pgpu {
@@ -46,6 +50,7 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
   static_assert(TILE % CG == 0 && CG % 2 == 0, "compensation group must divide the tile into source pairs");
   __shared__ __align__(16) float4 sP[2][TILE];
   __shared__ __align__(16) float4 sQ[2][TILE];
+  __shared__ __align__(16) float4 sN[TILE];  // n_s = (x_s - ref) x alpha_s, pair-interleaved like sP
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -63,9 +68,9 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
     const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
     const int64_t s1 = min(s0 + pe.chunk, pe.off + pe.n);
 
-    // targets: scalar copies for the near path and the fold, duplicated
-    // float2 copies for the packed far loop
-    float xt[TPT][3], at[TPT][3], hst[TPT], vt[TPT], h50[TPT];
+    // targets: positions duplicated into both float2 lanes (lane .x serves
+    // the scalar code); scalar strength, sigma^2/2 and volume
+    float at[TPT][3], hst[TPT], vt[TPT], h50[TPT];
     float2 X[TPT][3], AT3[TPT][3];
     float vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
     unsigned nfull = 0;  // pairs evaluated with the full (non-far) formula, self pairs included
@@ -75,12 +80,12 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
       ti = ti < tend ? ti : tend - 1;
       const float4 p = a.P[ti];
       const float4 q = a.Q[ti];
-      xt[k][0] = p.x; xt[k][1] = p.y; xt[k][2] = p.z; hst[k] = p.w;
+      hst[k] = p.w;
       h50[k] = kFarU * p.w;
       at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
-        X[k][m] = make_float2(xt[k][m], xt[k][m]);
+        X[k][m] = dup2(m == 0 ? p.x : m == 1 ? p.y : p.z);
         // -3 alpha_t: the far limit's F' = -3 r^5 with the constant folded in
         AT3[k][m] = make_float2(-3.f * at[k][m], -3.f * at[k][m]);
         vh[k][m] = 0.f; vl[k][m] = 0.f; dh[k][m] = 0.f; dl[k][m] = 0.f;
@@ -91,7 +96,7 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
     WarpBox tb;
     tb.init();
 #pragma unroll
-    for (int k = 0; k < TPT; ++k) tb.add(xt[k][0], xt[k][1], xt[k][2], hst[k]);
+    for (int k = 0; k < TPT; ++k) tb.add(X[k][0].x, X[k][1].x, X[k][2].x, hst[k]);
     tb.reduce();
 
     // Stage source j into buffer b at its pair-interleaved place.
@@ -118,6 +123,26 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
       if (sb + TILE < s1) stage(buf ^ 1, sb + TILE + tid);
       cp_async_commit();
       cp_async_wait<1>();
+      __syncthreads();
+
+      // Positions relative to the tile's first source, ref: with n_s =
+      // (x_s - ref) x alpha_s and X' = x_t - ref, alpha_s x d = alpha_s x X' +
+      // n_s, so the far loop sums q alpha_s and q n_s and forms the velocity
+      // (sum q alpha_s) x X' + sum q n_s once per group; the stretching's
+      // alpha_t . w becomes alpha_s . (X' x alpha_t) + n_s . alpha_t.  Keeping
+      // ref inside the tile bounds the cancellation by the tile's extent.
+      const float *fp = reinterpret_cast<const float *>(&sP[buf][0]);
+      const float rx = fp[0], ry = fp[2], rz = fp[4];
+      {
+        const float *fq = reinterpret_cast<const float *>(&sQ[buf][0]);
+        const int e = (tid >> 1) * 8 + (tid & 1);
+        const float px = fp[e] - rx, py = fp[e + 2] - ry, pz = fp[e + 4] - rz;
+        const float ax = fq[e], ay = fq[e + 2], az = fq[e + 4];
+        float *fn = reinterpret_cast<float *>(sN);
+        fn[e] = py * az - pz * ay;
+        fn[e + 2] = pz * ax - px * az;
+        fn[e + 4] = px * ay - py * ax;
+      }
       __syncthreads();
 
       // Every pair of this warp's targets with this tile's sources is far
@@ -150,12 +175,25 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
           }
         }
         if (far_tile) {
+          // B3 = X' x (-3 alpha_t), duplicated into both lanes (per group, so
+          // that it is live only in this loop)
+          float2 B3[TPT][3];
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            const float xr0 = X[k][0].x - rx, xr1 = X[k][1].x - ry, xr2 = X[k][2].x - rz;
+            const float c0 = AT3[k][0].x, c1 = AT3[k][1].x, c2 = AT3[k][2].x;
+            B3[k][0] = dup2(xr1 * c2 - xr2 * c1);
+            B3[k][1] = dup2(xr2 * c0 - xr0 * c2);
+            B3[k][2] = dup2(xr0 * c1 - xr1 * c0);
+          }
 #pragma unroll kF32Unroll
           for (int r = g; r < g + CG / 2; ++r) {
             const float4 pa = sP[buf][2 * r], pb = sP[buf][2 * r + 1];
             const float4 qa = sQ[buf][2 * r], qb = sQ[buf][2 * r + 1];
+            const float4 na = sN[2 * r], nb = sN[2 * r + 1];
             const float2 px = make_float2(pa.x, pa.y), py = make_float2(pa.z, pa.w), pz = make_float2(pb.x, pb.y);
             const float2 ax = make_float2(qa.x, qa.y), ay = make_float2(qa.z, qa.w), az = make_float2(qb.x, qb.y);
+            const float2 nx = make_float2(na.x, na.y), ny = make_float2(na.z, na.w), nz = make_float2(nb.x, nb.y);
 #pragma unroll
             for (int k = 0; k < TPT; ++k) {
               // d = x_t - x_s (exact-rounded, as a subtraction)
@@ -165,29 +203,29 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
               float2 r2 = __fmul2_rn(dx, dx);
               r2 = __ffma2_rn(dy, dy, r2);
               r2 = __ffma2_rn(dz, dz, r2);
-              // far limit: q' = r^3, F' = -3 r^5 (the -3 is in AT3), no diffusion
+              // far limit: q' = r^3, F' = -3 r^5 (the -3 is in AT3 and B3), no diffusion
               const float2 ir = make_float2(fast_rsqrt(r2.x), fast_rsqrt(r2.y));
               const float2 A = __fmul2_rn(ir, ir);
               const float2 qq = __fmul2_rn(A, ir);
               const float2 qA = __fmul2_rn(qq, A);
-              // w = alpha_s x d
-              const float2 wx = make_float2(ay.x * dz.x - az.x * dy.x, ay.y * dz.y - az.y * dy.y);
-              const float2 wy = make_float2(az.x * dx.x - ax.x * dz.x, az.y * dx.y - ax.y * dz.y);
-              const float2 wz = make_float2(ax.x * dy.x - ay.x * dx.x, ax.y * dy.y - ay.y * dx.y);
-              sv[k][0] = __ffma2_rn(qq, wx, sv[k][0]);
-              sv[k][1] = __ffma2_rn(qq, wy, sv[k][1]);
-              sv[k][2] = __ffma2_rn(qq, wz, sv[k][2]);
-              // F (alpha_t . w) d
-              float2 dot = __fmul2_rn(AT3[k][0], wx);
-              dot = __ffma2_rn(AT3[k][1], wy, dot);
-              dot = __ffma2_rn(AT3[k][2], wz, dot);
+              // sum q alpha_s and sum q n_s (the velocity is formed at the fold)
+              sp[k][0] = __ffma2_rn(qq, ax, sp[k][0]);
+              sp[k][1] = __ffma2_rn(qq, ay, sp[k][1]);
+              sp[k][2] = __ffma2_rn(qq, az, sp[k][2]);
+              sv[k][0] = __ffma2_rn(qq, nx, sv[k][0]);
+              sv[k][1] = __ffma2_rn(qq, ny, sv[k][1]);
+              sv[k][2] = __ffma2_rn(qq, nz, sv[k][2]);
+              // F (alpha_t . w) d, alpha_t . w = alpha_s . (X' x alpha_t) + n_s . alpha_t
+              float2 dot = __fmul2_rn(ax, B3[k][0]);
+              dot = __ffma2_rn(ay, B3[k][1], dot);
+              dot = __ffma2_rn(az, B3[k][2], dot);
+              dot = __ffma2_rn(nx, AT3[k][0], dot);
+              dot = __ffma2_rn(ny, AT3[k][1], dot);
+              dot = __ffma2_rn(nz, AT3[k][2], dot);
               const float2 fd = __fmul2_rn(qA, dot);
               sd[k][0] = __ffma2_rn(fd, dx, sd[k][0]);
               sd[k][1] = __ffma2_rn(fd, dy, sd[k][1]);
               sd[k][2] = __ffma2_rn(fd, dz, sd[k][2]);
-              sp[k][0] = __ffma2_rn(qq, ax, sp[k][0]);
-              sp[k][1] = __ffma2_rn(qq, ay, sp[k][1]);
-              sp[k][2] = __ffma2_rn(qq, az, sp[k][2]);
             }
           }
         } else {
@@ -196,7 +234,7 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
           auto one = [&](float sx, float sy, float sz, float shs, float qx, float qy, float qz, float qv) {
 #pragma unroll
             for (int k = 0; k < TPT; ++k) {
-              const float dx = xt[k][0] - sx, dy = xt[k][1] - sy, dz = xt[k][2] - sz;
+              const float dx = X[k][0].x - sx, dy = X[k][1].x - sy, dz = X[k][2].x - sz;
               const float r2 = dx * dx + dy * dy + dz * dz;
               // far test r^2 >= 50 (hs_t + hs_s) as one FMA against the
               // target's precomputed 50 hs_t
@@ -244,6 +282,14 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
             svs[m] = sv[k][m].x + sv[k][m].y;
             sds[m] = sd[k][m].x + sd[k][m].y;
             sps[m] = sp[k][m].x + sp[k][m].y;
+          }
+          if (far_tile) {
+            // velocity = (sum q alpha_s) x X' + sum q n_s
+            const float xr0 = X[k][0].x - rx, xr1 = X[k][1].x - ry, xr2 = X[k][2].x - rz;
+            const float n0 = svs[0], n1 = svs[1], n2 = svs[2];
+            svs[0] = sps[1] * xr2 - sps[2] * xr1 + n0;
+            svs[1] = sps[2] * xr0 - sps[0] * xr2 + n1;
+            svs[2] = sps[0] * xr1 - sps[1] * xr0 + n2;
           }
           // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t)
           const float ex = at[k][1] * sps[2] - at[k][2] * sps[1] + sds[0] + a.nu2 * sdv[k][0];
