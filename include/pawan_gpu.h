@@ -133,6 +133,18 @@ int pgpu_set_target_range(pgpu_ctx *ctx, int32_t system, int64_t first, int64_t 
 int pgpu_stage(pgpu_ctx *ctx, int scheme, int stage, double dt);
 int pgpu_records(pgpu_ctx *ctx, int32_t system, void **P, void **Q);
 
+/* Replaces: __interaction::influence (interaction.cpp:212-260, with
+ * INFLUENCE / SELFINFLUENCE, interaction_utils.h:626-703), which
+ * __interaction::resolve (interaction.cpp:59-62) calls: the vorticity field
+ * k_t = sum_s zeta(rho_ts, sigma_ts) alpha_s at every particle, from every
+ * particle of its system (the particle itself included).  Always in FP64,
+ * from the FP64 state, in both precision modes: PAWAN's strength solve
+ * (__resolve::rebuild, resolve.cpp:12-63) LU-solves a matrix of these fields
+ * and needs their digits.  pgpu_get_vorticity_field then copies one wake's
+ * rows (n x 3, row-major) to the host (PAWAN: the wake's _vorticityfield). */
+int pgpu_influence(pgpu_ctx *ctx);
+int pgpu_get_vorticity_field(pgpu_ctx *ctx, int32_t wake, double *field);
+
 /* Replaces: __interaction::diagnose (interaction.cpp:64-194) for one system.
  * out[15] = total vorticity(3), linear impulse(3), angular impulse(3),
  * helicity, enstrophy, enstrophyF, kinetic energy, kinetic energyF, Zc - the

@@ -77,6 +77,7 @@ def ref_lib():
         lib.ref_step.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
         lib.ref_diagnose.argtypes = [C.c_void_p, _dp]
         lib.ref_getvi.argtypes = [C.c_void_p, _dp, _dp]
+        lib.ref_influence.argtypes = [C.c_void_p, _dp]
         lib.ref_integrate.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]
         lib.ref_wtime.restype = C.c_double
         _ref = lib
@@ -133,6 +134,13 @@ class RefSystem:
         self.lib.ref_diagnose(self.h, _p(out))
         return out
 
+    def vorticity_field(self) -> np.ndarray:
+        """PAWAN's resolve()/influence(): the vorticity field of every particle,
+        wakes concatenated in order (sum(ns) x 3)."""
+        out = np.zeros((int(sum(self.ns)), 3))
+        self.lib.ref_influence(self.h, _p(out))
+        return out
+
     def getvi(self, r) -> np.ndarray:
         r = _c(r)
         out = np.zeros(3)
@@ -151,6 +159,7 @@ def restate_lib():
         lib.rs_step.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int64, _dp, _dp, _dp, _dp, C.c_double]
         lib.rs_diagnose.argtypes = [C.c_int, _i64p, _dp, _dp, _dp, C.c_double, _dp, _dp]
         lib.rs_getvi.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp]
+        lib.rs_vorticity_field.argtypes = [C.c_int64, _dp, _dp, _dp, _i64p, C.c_int64, _dp]
         lib.rs_threads.restype = C.c_int
         _rs = lib
     return _rs
@@ -171,6 +180,20 @@ def restate_rates(w, nu: float, targets=None):
     a = np.zeros((nt, 3))
     lib.rs_rates(w.n, _p(pos), _p(al), _p(sg), _p(vo), float(nu), tp, nt, _p(v), _p(a))
     return v, a
+
+
+def restate_vorticity_field(w, targets=None) -> np.ndarray:
+    """Vorticity field (n x 3) of the listed targets (all if None) from all particles of ``w``."""
+    lib = restate_lib()
+    pos, al, sg = _c(w.pos), _c(w.alpha), _c(w.sigma)
+    if targets is None:
+        nt, tp = w.n, None
+    else:
+        t = _c(targets, np.int64)
+        nt, tp = t.shape[0], t.ctypes.data_as(_i64p)
+    out = np.zeros((nt, 3))
+    lib.rs_vorticity_field(w.n, _p(pos), _p(al), _p(sg), tp, nt, _p(out))
+    return out
 
 
 def restate_step(w, nu: float, scheme: str, dt: float, nsteps: int):

@@ -148,6 +148,17 @@ void ref_get_wake(void *hp, int w, double *pos, double *alpha) {
 
 void ref_solve(void *hp) { ((handle *)hp)->S->sys()->solve(); }
 
+// PAWAN's resolve() (interaction.cpp:59-62: influence() over all wakes), then
+// each wake's _vorticityfield, wakes concatenated in order.
+void ref_influence(void *hp, double *field) {
+  handle *h = (handle *)hp;
+  h->S->sys()->resolve();
+  size_t row = 0;
+  for (oracle_wake *W : h->wakes)
+    for (size_t i = 0; i < W->_numParticles; ++i, ++row)
+      for (int k = 0; k < 3; ++k) field[3 * row + k] = gsl_matrix_get(W->_vorticityfield, i, k);
+}
+
 void ref_get_rates(void *hp, int w, double *vel, double *dalpha) {
   oracle_wake *W = ((handle *)hp)->wakes[w];
   for (size_t i = 0; i < W->_numParticles; ++i)

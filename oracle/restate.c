@@ -227,4 +227,29 @@ void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *s
   for (int k = 0; k < 3; ++k) out[k] = u[k];
 }
 
+/* Vorticity field of the listed targets (all if NULL), PAWAN's influence()
+ * (interaction.cpp:212-260; INFLUENCE / SELFINFLUENCE, interaction_utils.h:
+ * 626-703): k_t = sum_s ZETASIG(rho_ts, sigma_ts) alpha_s over every particle
+ * s, the target itself included (rho = 0, sigma_tt = sigma_t), with
+ * sigma_ts = sqrt((sigma_t^2 + sigma_s^2) / 2) and ZETASIG (gaussian.h:20-23)
+ * = exp(-rho^2 / (2 sigma^2)) / sigma^3 / (2 pi)^1.5. */
+void rs_vorticity_field(int64_t n, const double *pos, const double *alpha, const double *sigma,
+                        const int64_t *targets, int64_t nt, double *field) {
+  if (!targets) nt = n;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < nt; ++i) {
+    const int64_t t = targets ? targets[i] : i;
+    double k[3] = {0.0, 0.0, 0.0};
+    for (int64_t s = 0; s < n; ++s) {
+      const double dx = pos[3 * t] - pos[3 * s], dy = pos[3 * t + 1] - pos[3 * s + 1], dz = pos[3 * t + 2] - pos[3 * s + 2];
+      const double rho = sqrt(dx * dx + dy * dy + dz * dz);
+      const double sg = sqrt(0.5 * (sigma[t] * sigma[t] + sigma[s] * sigma[s]));
+      const double rb = rho / sg;
+      const double z = exp(-0.5 * rb * rb) / pow(sg, 3.0) / pow(2.0 * M_PI, 1.5);
+      for (int m = 0; m < 3; ++m) k[m] += z * alpha[3 * s + m];
+    }
+    for (int m = 0; m < 3; ++m) field[3 * i + m] = k[m];
+  }
+}
+
 int rs_threads(void) { return omp_get_max_threads(); }

@@ -43,6 +43,10 @@ void rs_diagnose(int nw, const int64_t *offsets, const double *pos, const double
 void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *sigma,
               const double *r, double *out);
 
+/* Vorticity field k_t = sum_s zeta(rho_ts, sigma_ts) alpha_s of the listed
+ * targets (all if NULL), the target itself included (PAWAN's influence()). */
+void rs_vorticity_field(int64_t n, const double *pos, const double *alpha, const double *sigma,
+                        const int64_t *targets, int64_t nt, double *field);
 int rs_threads(void);
 
 #ifdef __cplusplus

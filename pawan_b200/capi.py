@@ -38,7 +38,7 @@ EXPORTS = [
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
     "pgpu_rates_noalloc", "pgpu_noalloc_last_error", "pgpu_set_target_range", "pgpu_stage", "pgpu_records",
-    "pgpu_sync_timeout", "pgpu_set_timing",
+    "pgpu_sync_timeout", "pgpu_set_timing", "pgpu_influence", "pgpu_get_vorticity_field",
 ]
 
 
@@ -148,6 +148,8 @@ def load(build_if_missing: bool = False):
         "pgpu_records": (C.c_int, [vp, C.c_int32, C.POINTER(vp), C.POINTER(vp)]),
         "pgpu_sync_timeout": (C.c_int, [vp, C.c_double]),
         "pgpu_set_timing": (C.c_int, [vp, C.c_int]),
+        "pgpu_influence": (C.c_int, [vp]),
+        "pgpu_get_vorticity_field": (C.c_int, [vp, C.c_int32, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -306,6 +308,14 @@ class Context:
             self._ck(self.lib.pgpu_sync(self.h))
         else:
             self._ck(self.lib.pgpu_sync_timeout(self.h, float(timeout)))
+
+    def vorticity_field(self, wake: int = 0) -> np.ndarray:
+        """PAWAN's influence(): the vorticity field (n x 3) at the wake's particles
+        from all particles of its system; computes the field of every system."""
+        self._ck(self.lib.pgpu_influence(self.h))
+        out = np.zeros((self.num_particles(wake), 3))
+        self._ck(self.lib.pgpu_get_vorticity_field(self.h, wake, _p(out)))
+        return out
 
     def diagnose(self, system: int = 0):
         out = np.zeros(15)

@@ -667,6 +667,100 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
   }
 }
 
+// Vorticity field at every particle, PAWAN's influence() (interaction.cpp:
+// 212-260; INFLUENCE and SELFINFLUENCE, interaction_utils.h:626-703):
+//   k_t = sum_s zeta(rho_ts, sigma_ts) alpha_s,  the self term s = t included,
+//   zeta = exp(-rho^2 / (2 sigma^2)) / (sigma^3 (2 pi)^1.5)   (ZETASIG, gaussian.h:20-23)
+//   sigma_ts^2 = (sigma_t^2 + sigma_s^2) / 2.
+// Always FP64, from the FP64 state (x0, sig) rather than the mode's source
+// records: PAWAN's strength solve (resolve.cpp:12-63) LU-solves a matrix of
+// these fields, whose conditioning (~1e6 for its vortex rings) turns FP32
+// rounding into percent-level strength errors.  Per target and source chunk,
+// row sums go to partial[c][0..2][t]; field_reduce_kernel adds the chunks.
+// A warp whose pairs all have u > 1500 skips the exponential: e^{-750} is
+// below the smallest double, so the term is exactly zero anyway.
+struct FieldArgs {
+  const double *x0;   // [6][cap] state
+  const double *sig;  // [cap]
+  double *partial;    // [nch][6][cap]
+  const PlanEntry *plan;
+  int nsys;
+  int nch;
+  int64_t cap;
+  unsigned int *counters;
+};
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) field_kernel(FieldArgs a) {
+  __shared__ __align__(16) double4 sP[BLOCK];  // (x, y, z, sigma^2 / 2)
+  __shared__ __align__(16) double4 sQ[BLOCK];  // (alpha, 0)
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const int64_t cap = a.cap;
+  const int64_t total = a.plan[a.nsys].item_start;
+  int64_t item;
+  while (next_item(a.counters, total, item, &s_item)) {
+    const int si = find_plan(a.plan, a.nsys, item);
+    const PlanEntry pe = a.plan[si];
+    const int64_t local = item - pe.item_start;
+    const int64_t tile = local / a.nch;
+    const int c = (int)(local - tile * a.nch);
+    const int64_t tend = pe.off + pe.n;
+    const int64_t t = min(pe.off + tile * BLOCK + tid, tend - 1);
+    const bool valid = pe.off + tile * BLOCK + tid < tend;
+    const int64_t s0 = pe.off + (int64_t)c * pe.chunk;
+    const int64_t s1 = min(s0 + pe.chunk, tend);
+    const double xt = a.x0[t], yt = a.x0[cap + t], zt = a.x0[2 * cap + t];
+    const double hst = 0.5 * a.sig[t] * a.sig[t];
+    double k[3] = {0, 0, 0};
+    for (int64_t sb = s0; sb < s1; sb += BLOCK) {
+      __syncthreads();
+      const int64_t j = sb + tid;
+      if (j < s1) {
+        const double sj = a.sig[j];
+        sP[tid] = make_double4(a.x0[j], a.x0[cap + j], a.x0[2 * cap + j], 0.5 * sj * sj);
+        sQ[tid] = make_double4(a.x0[3 * cap + j], a.x0[4 * cap + j], a.x0[5 * cap + j], 0.0);
+      } else {
+        sP[tid] = pad_P<double>();
+        sQ[tid] = pad_Q<double>();
+      }
+      __syncthreads();
+      const int cnt = (int)min((int64_t)BLOCK, s1 - sb);
+      for (int jj = 0; jj < cnt; ++jj) {
+        const double4 p = sP[jj], q = sQ[jj];
+        const double dx = xt - p.x, dy = yt - p.y, dz = zt - p.z;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double s2 = hst + p.w;
+        double z = 0.0;
+        const bool live = r2 < 1500.0 * s2;
+        if (__any_sync(0xffffffffu, live)) z = kInv2Pi15 / (s2 * sqrt(s2)) * exp(-0.5 * r2 / s2);
+        k[0] += z * q.x;
+        k[1] += z * q.y;
+        k[2] += z * q.z;
+      }
+    }
+    if (valid) {
+      double *o = a.partial + (int64_t)c * 6 * cap + t;
+      o[0] = k[0];
+      o[cap] = k[1];
+      o[2 * cap] = k[2];
+    }
+  }
+}
+
+// field[m][i] = sum over chunks of partial[c][m][i], m = 0..2; components 3..5
+// of field are zero (the [6][cap] layout the row gather expects).
+static __global__ void field_reduce_kernel(const double *partial, int nch, int64_t cap, double *field) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cap; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int m = 0; m < 3; ++m) {
+      double v = 0.0;
+      for (int c = 0; c < nch; ++c) v += partial[((int64_t)c * 6 + m) * cap + i];
+      field[m * cap + i] = v;
+      field[(3 + m) * cap + i] = 0.0;
+    }
+  }
+}
+
 // Per-wake O(N) diagnostics and the reduction of the quadratic row sums, FP64.
 // Fields (per CTA partial, summed on the host in CTA order):
 //   0-2 sum alpha, 3-5 sum x x alpha, 6-8 sum x x (x x alpha), 9 Zc numerator,

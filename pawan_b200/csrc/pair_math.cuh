@@ -46,6 +46,7 @@ template <typename T> using v4_t = typename V4<T>::type;
 constexpr double kK1 = 0.7978845608028654;       // sqrt(2/pi)
 constexpr double kInv4Pi = 0.07957747154594767;  // 1/(4 pi)
 constexpr double kNegHalfLog2e = -0.7213475204444817;  // -0.5 / ln 2
+constexpr double kInv2Pi15 = 0.06349363593424097;     // (2 pi)^-1.5
 
 // Series coefficients S_k = (-1)^k/(2^k k!(2k+3)), T_m = (-1)^m/(2^m m!(2m+5)).
 #define PGPU_S0 0.3333333333333333

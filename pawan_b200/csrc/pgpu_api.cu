@@ -83,7 +83,8 @@ struct pgpu_ctx {
   double *partial = nullptr, *stage = nullptr, *d_diag = nullptr;
   void *P = nullptr, *Q = nullptr;
   int64_t *d_sysoff = nullptr, *d_sysn = nullptr, *d_syst = nullptr;
-  PlanEntry *d_plan = nullptr, *d_plan_diag = nullptr;
+  PlanEntry *d_plan = nullptr, *d_plan_diag = nullptr, *d_plan_field = nullptr;
+  double *d_field = nullptr;  // [6][cap] vorticity field (components 0..2), allocated by pgpu_influence
   unsigned int *d_counters = nullptr;
   unsigned long long *d_nfull = nullptr;
   int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
@@ -206,6 +207,7 @@ int freeze(pgpu_ctx *c) {
   if ((r = alloc((void **)&c->d_syst, 2 * ns * sizeof(int64_t)))) return r;
   if ((r = alloc((void **)&c->d_plan, (ns + 1) * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_plan_diag, 2 * sizeof(PlanEntry)))) return r;
+  if ((r = alloc((void **)&c->d_plan_field, (ns + 1) * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_counters, 4 * sizeof(unsigned int)))) return r;
   if ((r = alloc((void **)&c->d_nfull, sizeof(unsigned long long)))) return r;
   if ((r = alloc((void **)&c->d_flag, sizeof(int)))) return r;
@@ -494,8 +496,8 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
-                  c->d_sysoff, c->d_sysn, c->d_syst, c->d_plan, c->d_plan_diag, c->d_counters, c->d_nfull,
-                  c->d_flag};
+                  c->d_sysoff, c->d_sysn, c->d_syst, c->d_plan, c->d_plan_diag, c->d_plan_field, c->d_field,
+                  c->d_counters, c->d_nfull, c->d_flag};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
@@ -817,6 +819,58 @@ int pgpu_sync(pgpu_ctx *c) {
     }
   }
   return PGPU_OK;
+}
+
+int pgpu_influence(pgpu_ctx *c) {
+  if (!c) return PGPU_EINVAL;
+  NvtxRange nvtx("pgpu_influence");
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  int r = check_contiguous(c);
+  if (r) return r;
+  if (!c->d_field) {
+    const cudaError_t e = cudaMalloc((void **)&c->d_field, 6 * (size_t)c->cap * sizeof(double));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      c->d_field = nullptr;
+      return fail(c, PGPU_ENOMEM, "cudaMalloc of the vorticity field failed: %s", cudaGetErrorString(e));
+    }
+  }
+  // every particle of every system is a target, 256-target tiles
+  const int shape = 2, block = 256;
+  int64_t tiles = 0;
+  std::vector<int> all(c->sys.size());
+  for (size_t s = 0; s < all.size(); ++s) {
+    all[s] = (int)s;
+    tiles += ceil_div(sys_n(c, (int)s), block);
+  }
+  const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxChunks, ceil_div(8LL * c->sms, std::max<int64_t>(1, tiles))));
+  std::vector<PlanEntry> plan = build_plan(c, all, shape, nch, false);
+  plan.resize(c->sys.size() + 1, plan.back());
+  CK(cudaMemcpyAsync(c->d_plan_field, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));  // the plan vector is pageable host memory
+  if (plan.size() > 1 && plan.front().n > 0) {
+    int grid = 0;
+    FieldArgs a{c->x0, c->sig, c->partial, c->d_plan_field, (int)c->sys.size(), nch, c->cap, c->d_counters};
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, field_kernel<256>, block, 0));
+    field_kernel<256><<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
+    CK(cudaGetLastError());
+    c->launches++;
+  }
+  const int rg = (int)std::min<int64_t>(ceil_div(c->cap, 256), 16LL * c->sms);
+  field_reduce_kernel<<<rg, 256, 0, c->st>>>(c->partial, nch, c->cap, c->d_field);
+  CK(cudaGetLastError());
+  c->launches++;
+  return PGPU_OK;
+}
+
+int pgpu_get_vorticity_field(pgpu_ctx *c, int32_t wake, double *field) {
+  int r = wake_ok(c, wake);
+  if (r) return r;
+  if (!field) return fail(c, PGPU_EINVAL, "null output array");
+  if (!c->d_field) return fail(c, PGPU_EINVAL, "no vorticity field was computed (pgpu_influence)");
+  const WakeRec &W = c->wakes[wake];
+  std::vector<double> zeros(3 * (size_t)W.n);
+  return download_rows(c, c->d_field, W, field, zeros.data());
 }
 
 int pgpu_set_timing(pgpu_ctx *c, int on) {

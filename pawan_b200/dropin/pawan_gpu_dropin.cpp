@@ -100,6 +100,18 @@ void __gpu::diagnose() {
   _Zc = out[14];
 }
 
+// __interaction::influence (interaction.cpp:212-260): zeroes every wake's
+// _vorticityfield and fills it with the field from all wakes (the particle
+// itself included, as SELFINFLUENCE adds it).
+void __gpu::influence() {
+  upload();
+  check(pgpu_influence(_ctx));
+  for (size_t k = 0; k < _wakes.size(); ++k) {
+    gsl_matrix_set_zero(_wakes[k]->_vorticityfield);
+    check(pgpu_get_vorticity_field(_ctx, _ids[k], _wakes[k]->_vorticityfield->data));
+  }
+}
+
 void __gpu::device_step(int scheme, double dt, int nsteps) {
   upload();
   check(pgpu_step(_ctx, scheme, dt, nsteps));

@@ -56,6 +56,14 @@ class __gpu : public __interaction {
   void probe(const double *pts, long npts, double *vel);
   pgpu_ctx *context() { return _ctx; }
 
+ protected:
+  // __interaction::influence (interaction.cpp:212-260), which resolve()
+  // (interaction.cpp:59-62) calls, and so PAWAN's __resolve::rebuild
+  // (resolve.cpp:12-63): the vorticity field of every particle from all
+  // wakes, on the device, written to each wake's _vorticityfield.  (The
+  // base's one- and two-wake overloads are private and not used here.)
+  void influence() override;
+
  private:
   void check(int rc) const;
   void layout();  // creates the device wakes on first use

@@ -7,6 +7,14 @@
 //   dropin_check ref|gpu|gpu64 rk4|rk3 <particles.bin> <dt> <nsteps> <out-prefix> [nu]
 //
 // particles.bin: int64 n, then n*3 positions, n*3 strengths, n radii, n volumes (FP64).
+//
+// A second mode runs PAWAN's strength solve __resolve::rebuild
+// (src/resolve/resolve.cpp:12-63) on one of PAWAN's own __vring wakes
+// (src/wake/vring.cpp), whose O(N^2) part is __interaction::resolve ->
+// influence(), with either backend, and writes the solved strengths (FP64)
+// to <out-prefix>.strengths:
+//
+//   dropin_check resolve ref|gpu|gpu64 <nLayers> <nAzi> <sigma> <out-prefix>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -17,6 +25,8 @@
 #include "pawan_gpu_dropin.h"
 #include "src/interaction/parallel.h"
 #include "src/io/io.h"
+#include "src/resolve/resolve.h"
+#include "src/wake/vring.h"
 
 namespace {
 
@@ -49,7 +59,41 @@ struct ref_parallel : public pawan::__parallel {
 
 }  // namespace
 
+int run_resolve(int argc, char **argv) {
+  if (argc < 7) {
+    fprintf(stderr, "usage: %s resolve ref|gpu|gpu64 nLayers nAzi sigma out\n", argv[0]);
+    return 2;
+  }
+  const std::string backend = argv[2];
+  pawan::__wake *W = new pawan::__vring(1.0, 0.1, atoi(argv[3]), atoi(argv[4]), atof(argv[5]));
+  path_io io(argv[6]);
+  pawan::__interaction *S = nullptr;
+  if (backend == "ref") {
+    S = new ref_parallel(W, 1e-4);
+  } else {
+    pgpu_config cfg;
+    pgpu_config_default(&cfg);
+    cfg.nu = 1e-4;
+    cfg.precision = backend == "gpu64" ? PGPU_FP64 : PGPU_FP32C;
+    S = new pawan::__gpu(W, cfg);
+  }
+  pawan::__resolve R;
+  R.rebuild(S, &io);
+  gsl_vector *st = gsl_vector_calloc(S->_size);
+  S->getStates(st);
+  FILE *f = fopen((std::string(argv[6]) + ".strengths").c_str(), "wb");
+  if (!f) return 3;
+  fwrite(st->data, sizeof(double), st->size, f);
+  fclose(f);
+  gsl_vector_free(st);
+  fflush(NULL);
+  delete S;
+  delete W;
+  return 0;
+}
+
 int main(int argc, char **argv) {
+  if (argc > 1 && std::string(argv[1]) == "resolve") return run_resolve(argc, argv);
   if (argc < 7) {
     fprintf(stderr, "usage: %s ref|gpu|gpu64 rk4|rk3 particles.bin dt nsteps out [nu]\n", argv[0]);
     return 2;

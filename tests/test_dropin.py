@@ -98,3 +98,33 @@ def test_dropin_matches_reference_in_pawan_time_loop(gpu, driver, tmp_path, ref_
     np.testing.assert_allclose(dgot[:, 4:10], dref[:, 4:10], rtol=max(tol, 1e-10),
                                atol=max(tol, 1e-10) * np.abs(dref[:, 4:10]).max())
     np.testing.assert_allclose(dgot[:, 13:15], dref[:, 13:15], rtol=max(tol, 1e-10))
+
+
+def _resolve(driver, out, backend):
+    r = subprocess.run([str(driver), "resolve", backend, "3", "49", "0.1924", str(out)],
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return np.fromfile(str(out) + ".strengths")
+
+
+@pytest.fixture(scope="module")
+def resolved_ref(driver, tmp_path_factory):
+    """PAWAN's strength solve __resolve::rebuild (resolve.cpp:12-63) on its own
+    fusion-case ring __vring(1, 0.1, 3, 49, 0.1924), with __parallel."""
+    if not O.ref_available():
+        pytest.skip("oracle/_ref/libpawanref.so is not built (make -C oracle)")
+    return _resolve(driver, tmp_path_factory.mktemp("resolve") / "ref", "ref")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["gpu64", "gpu"])
+def test_dropin_resolve_matches_reference(gpu, driver, resolved_ref, tmp_path, mode):
+    """The same rebuild with __gpu: every column's influence() runs on the
+    device, in FP64 in both modes; the solved strengths match PAWAN's.  The
+    influence matrix's condition number (~1e6) turns the fields' last-digit
+    differences into ~1e-9 of the strengths."""
+    tol = 1e-8
+    got = _resolve(driver, tmp_path / mode, mode)
+    err = np.abs(got - resolved_ref).max() / np.abs(resolved_ref).max()
+    print(f"resolve {mode}: max relative strength difference {err:.2e}")
+    assert err < tol

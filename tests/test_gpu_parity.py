@@ -396,3 +396,40 @@ def test_device_allocation_failure_is_reported(gpu):
         c2.solve()
         v, _ = c2.rates(k2)
         assert np.all(np.isfinite(v))
+
+
+@pytest.mark.parametrize("prec", PREC)
+def test_vorticity_field_vs_pawan_influence(gpu, ref_available, prec):
+    """pgpu_influence on two interacting wakes of one system against PAWAN's
+    own resolve()/influence() (interaction.cpp:59-62, 212-260)."""
+    w1 = cases.ring_stations(stations=40, seed=0)
+    w2 = cases.ring_stations(stations=30, R=0.7, seed=1)
+    with O.quiet():
+        R = O.RefSystem([w1, w2], 1e-4)
+        kref = R.vorticity_field()
+        R.close()
+    c, ids = ctx_with([w1, w2], prec, 1e-4)
+    k = np.vstack([c.vorticity_field(ids[0]), c.vorticity_field(ids[1])])
+    c.close()
+    assert O.rel_err(k, kref) < TOL[capi.FP64]  # FP64 in both modes
+
+
+def test_vorticity_field_separate_systems_and_1m_sampled(gpu):
+    """Systems do not see each other's particles; at N = 1M (an FP32C context;
+    the field is FP64 in both modes) 256 seeded targets match the FP64
+    restatement within the FP64 gate."""
+    w1 = cases.ring_stations(stations=40, seed=0)
+    w2 = cases.ring_stations(stations=30, R=0.7, seed=1)
+    c, ids = ctx_with([w1, w2], capi.FP32C, 1e-4, systems=[0, 1])
+    k1, k2 = c.vorticity_field(ids[0]), c.vorticity_field(ids[1])
+    c.close()
+    assert O.rel_err(k1, O.restate_vorticity_field(w1)) < TOL[capi.FP64]
+    assert O.rel_err(k2, O.restate_vorticity_field(w2)) < TOL[capi.FP64]
+    w = cases.ring_gaussian()
+    c, ids = ctx_with([w], capi.FP32C, 1e-4)
+    k = c.vorticity_field(ids[0])
+    c.close()
+    rows = np.sort(np.random.default_rng(13).choice(w.n, 256, replace=False))
+    e = O.rel_err(k[rows], O.restate_vorticity_field(w, targets=rows))
+    print(f"1M ring vorticity field, 256 sampled targets: {e:.2e}")
+    assert e < TOL[capi.FP64]

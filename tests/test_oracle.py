@@ -118,3 +118,16 @@ def test_reference_integrate_files_present():
     assert len(wake) == 4 * rec
     # .diagnosis: nu, then per record t + 15 doubles
     assert len(diag) == 8 + 4 * 16 * 8
+
+
+def test_restated_vorticity_field_matches_pawan_influence(ref_available):
+    """The FP64 restatement of influence() against PAWAN's own resolve() on two
+    interacting wakes (interaction.cpp:212-260)."""
+    w1 = cases.ring_stations(stations=40, seed=0)
+    w2 = cases.ring_stations(stations=30, R=0.7, seed=1)
+    with O.quiet():
+        R = O.RefSystem([w1, w2], 1e-4)
+        k = R.vorticity_field()
+        R.close()
+    kr = O.restate_vorticity_field(cases.Wake.concat([w1, w2]))
+    assert O.rel_err(kr, k) < 1e-13
