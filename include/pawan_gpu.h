@@ -36,6 +36,12 @@ extern "C" {
 #define PGPU_FP32C 0 /* FP32 pair terms, compensated per-target sums, FP64 state */
 #define PGPU_FP64 1  /* FP64 throughout */
 
+/* Regularisation kernel.  PAWAN picks one at compile time with the
+ * HIGHORDER / GAUSSIAN macros of src/interaction/interaction_utils.h:13-20;
+ * here it is a per-context setting. */
+#define PGPU_KERNEL_GAUSSIAN 0  /* src/interaction/gaussian.h (PAWAN's default) */
+#define PGPU_KERNEL_HIGHORDER 1 /* src/interaction/highorder.h, high-order algebraic */
+
 #define PGPU_EULER 0
 #define PGPU_RK3 1
 #define PGPU_RK4 2
@@ -52,6 +58,10 @@ typedef struct pgpu_config {
   int tpt;         /* pair-kernel targets per thread; 0 = autotuned default */
   int chunks;      /* source chunks per system (1..16); 0 = automatic */
   int use_graphs;  /* capture each time step in a CUDA graph (default 1) */
+  int kernel;      /* PGPU_KERNEL_GAUSSIAN (default) or PGPU_KERNEL_HIGHORDER; rates,
+                      diagnostics (enstrophy and enstrophyF are non-zero only for the
+                      high-order kernel, as in PAWAN), probes and the vorticity field all
+                      use it.  The far-field surrogate supports the Gaussian kernel only. */
 } pgpu_config;
 
 /* Fills cfg with defaults (FP32C, device 0, nu = 1.56e-5 as __interaction(),
@@ -150,7 +160,8 @@ int pgpu_get_vorticity_field(pgpu_ctx *ctx, int32_t wake, double *field);
  * helicity, enstrophy, enstrophyF, kinetic energy, kinetic energyF, Zc - the
  * record of writediagnosis (interaction.cpp:325-335); vbi[3] = velocity
  * induced at the origin (may be NULL).  Enstrophy terms are identically zero
- * for the Gaussian kernel (gaussian.h:69-92).  Zc follows PAWAN: the last wake
+ * for the Gaussian kernel (gaussian.h:69-92) and follow ENST / ENSTF
+ * (highorder.h:71-110) for the high-order kernel.  Zc follows PAWAN: the last wake
  * with non-zero weight wins, else the previous value is kept. */
 int pgpu_diagnose(pgpu_ctx *ctx, int32_t system, double *out, double *vbi);
 
@@ -229,7 +240,8 @@ typedef struct pgpu_surrogate_stats {
 } pgpu_surrogate_stats;
 
 void pgpu_surrogate_config_default(pgpu_surrogate_config *cfg);
-/* Enables the surrogate for `system`, which must be the context's only system. */
+/* Enables the surrogate for `system`, which must be the context's only system.
+ * Refused (PGPU_EINVAL) for a context with the high-order kernel. */
 int pgpu_surrogate_enable(pgpu_ctx *ctx, int32_t system, const pgpu_surrogate_config *cfg);
 int pgpu_surrogate_disable(pgpu_ctx *ctx);
 int pgpu_surrogate_get_stats(pgpu_ctx *ctx, pgpu_surrogate_stats *stats);

@@ -4,7 +4,9 @@ Two tiers, both built by ``oracle/Makefile`` into ``oracle/_ref/``:
 
 * ``RefSystem`` drives PAWAN's own C++ classes (``__interaction`` /
   ``__parallel``, ``__rk3`` / ``__rk4``, ``__integration::integrate``) compiled
-  from the unmodified PAWAN sources against the project's GSL-subset shim.
+  from the unmodified PAWAN sources against the project's GSL-subset shim,
+  once with PAWAN's default Gaussian kernel (``libpawanref.so``) and once with
+  its high-order algebraic kernel (``libpawanref_ho.so``).
 * ``restate_*`` call the FP64 CPU restatement (``oracle/restate.c``), validated
   against ``RefSystem`` at small N and used for sampled checks at large N.
 
@@ -36,8 +38,15 @@ def _c(a, dtype=np.float64) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-_ref = None
+_ref = {}
 _rs = None
+# Regularisation kernels, as the C ABI's PGPU_KERNEL_* values.
+KERNELS = {"gaussian": 0, "highorder": 1}
+_REF_LIBS = {0: "libpawanref.so", 1: "libpawanref_ho.so"}
+
+
+def kernel_id(kernel) -> int:
+    return KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
 
 
 @contextlib.contextmanager
@@ -59,14 +68,14 @@ def quiet():
         os.close(devnull)
 
 
-def ref_available() -> bool:
-    return (REF_DIR / "libpawanref.so").exists()
+def ref_available(kernel="gaussian") -> bool:
+    return (REF_DIR / _REF_LIBS[kernel_id(kernel)]).exists()
 
 
-def ref_lib():
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(str(REF_DIR / "libpawanref.so"))
+def ref_lib(kernel="gaussian"):
+    k = kernel_id(kernel)
+    if k not in _ref:
+        lib = C.CDLL(str(REF_DIR / _REF_LIBS[k]))
         lib.ref_create.restype = C.c_void_p
         lib.ref_create.argtypes = [C.c_int, _i64p, C.c_double, C.c_int]
         lib.ref_destroy.argtypes = [C.c_void_p]
@@ -80,18 +89,19 @@ def ref_lib():
         lib.ref_influence.argtypes = [C.c_void_p, _dp]
         lib.ref_integrate.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]
         lib.ref_wtime.restype = C.c_double
-        _ref = lib
-    return _ref
+        _ref[k] = lib
+    return _ref[k]
 
 
 SCHEMES = {"euler": 0, "rk3": 1, "rk4": 2}
 
 
 class RefSystem:
-    """One PAWAN ``__interaction`` (or ``__parallel``) holding several wakes."""
+    """One PAWAN ``__interaction`` (or ``__parallel``) holding several wakes,
+    from the PAWAN build of the given regularisation kernel."""
 
-    def __init__(self, wakes, nu: float, parallel: bool = True):
-        self.lib = ref_lib()
+    def __init__(self, wakes, nu: float, parallel: bool = True, kernel="gaussian"):
+        self.lib = ref_lib(kernel)
         self.ns = [w.n for w in wakes]
         n = np.array(self.ns, dtype=np.int64)
         self.h = self.lib.ref_create(len(wakes), n.ctypes.data_as(_i64p), float(nu), 1 if parallel else 0)
@@ -160,14 +170,22 @@ def restate_lib():
         lib.rs_diagnose.argtypes = [C.c_int, _i64p, _dp, _dp, _dp, C.c_double, _dp, _dp]
         lib.rs_getvi.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp]
         lib.rs_vorticity_field.argtypes = [C.c_int64, _dp, _dp, _dp, _i64p, C.c_int64, _dp]
+        lib.rs_set_kernel.argtypes = [C.c_int]
         lib.rs_threads.restype = C.c_int
         _rs = lib
     return _rs
 
 
-def restate_rates(w, nu: float, targets=None):
-    """(vel, dalpha) of the listed targets (all if None) from all particles of ``w``."""
+def _restate(kernel):
+    """The restatement library with its kernel switched to ``kernel``."""
     lib = restate_lib()
+    lib.rs_set_kernel(kernel_id(kernel))
+    return lib
+
+
+def restate_rates(w, nu: float, targets=None, kernel="gaussian"):
+    """(vel, dalpha) of the listed targets (all if None) from all particles of ``w``."""
+    lib = _restate(kernel)
     pos, al, sg, vo = _c(w.pos), _c(w.alpha), _c(w.sigma), _c(w.vol)
     if targets is None:
         nt = w.n
@@ -182,9 +200,9 @@ def restate_rates(w, nu: float, targets=None):
     return v, a
 
 
-def restate_vorticity_field(w, targets=None) -> np.ndarray:
+def restate_vorticity_field(w, targets=None, kernel="gaussian") -> np.ndarray:
     """Vorticity field (n x 3) of the listed targets (all if None) from all particles of ``w``."""
-    lib = restate_lib()
+    lib = _restate(kernel)
     pos, al, sg = _c(w.pos), _c(w.alpha), _c(w.sigma)
     if targets is None:
         nt, tp = w.n, None
@@ -196,17 +214,17 @@ def restate_vorticity_field(w, targets=None) -> np.ndarray:
     return out
 
 
-def restate_step(w, nu: float, scheme: str, dt: float, nsteps: int):
+def restate_step(w, nu: float, scheme: str, dt: float, nsteps: int, kernel="gaussian"):
     """Returns a new (pos, alpha) after ``nsteps`` steps."""
-    lib = restate_lib()
+    lib = _restate(kernel)
     pos, al = _c(w.pos).copy(), _c(w.alpha).copy()
     sg, vo = _c(w.sigma), _c(w.vol)
     lib.rs_step(SCHEMES[scheme], float(dt), int(nsteps), w.n, _p(pos), _p(al), _p(sg), _p(vo), float(nu))
     return pos, al
 
 
-def restate_diagnose(w, offsets=None, zc_prev: float = 0.0):
-    lib = restate_lib()
+def restate_diagnose(w, offsets=None, zc_prev: float = 0.0, kernel="gaussian"):
+    lib = _restate(kernel)
     if offsets is None:
         offsets = [0, w.n]
     off = _c(offsets, np.int64)
@@ -215,6 +233,15 @@ def restate_diagnose(w, offsets=None, zc_prev: float = 0.0):
     lib.rs_diagnose(len(offsets) - 1, off.ctypes.data_as(_i64p), _p(_c(w.pos)), _p(_c(w.alpha)),
                     _p(_c(w.sigma)), float(zc_prev), _p(out), _p(vbi))
     return out, vbi
+
+
+def restate_getvi(w, r, kernel="gaussian") -> np.ndarray:
+    """Velocity induced at point ``r`` by all particles of ``w``, each with its
+    own radius (PAWAN's getVi)."""
+    lib = _restate(kernel)
+    out = np.zeros(3)
+    lib.rs_getvi(w.n, _p(_c(w.pos)), _p(_c(w.alpha)), _p(_c(w.sigma)), _p(_c(r)), _p(out))
+    return out
 
 
 def restate_threads() -> int:

@@ -31,7 +31,9 @@
 #include "src/interaction/gaussian.h"
 
 // Five-argument kernel that interaction.cpp:465 calls; forwards to the
-// Gaussian six-argument kernel (gaussian.h:47-60).
+// six-argument kernel of the build: the Gaussian one (gaussian.h:47-60), or the
+// high-order one (highorder.h:54-61) when ref_highorder.h is force-included,
+// which also turns the include of gaussian.h above into an empty one.
 void KERNEL(const double &rho, const double &sigma, double &q, double &F, double &Z) {
   double n = 0.0;
   KERNEL(rho, sigma, q, F, Z, n);

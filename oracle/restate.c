@@ -19,22 +19,60 @@
 #define M_PI 3.14159265358979323846
 #endif
 
-/* Gaussian regularisation, src/interaction/gaussian.h:20-60 (ZETASIG, QSIG,
- * KERNEL): rb = rho/sigma,
- *   zeta = exp(-rb^2/2) / (sigma^3 (2 pi)^(3/2))
- *   phi  = erf(rb / sqrt 2) / (4 pi sigma^3)
- *   q    = (phi/rb - zeta) / rb^2
- *   F    = (zeta - 3 q) / rho^2
- * The diffusion kernel eta is zeta itself (gaussian.h:58). */
-static inline void kernel_terms(double rho, double sigma, double *q, double *F, double *Z) {
+/* Kernel of the whole restatement (rs_set_kernel): 0 Gaussian, 1 high-order
+ * algebraic.  PAWAN fixes it at compile time (interaction_utils.h:13-20). */
+static int g_kernel = 0;
+
+void rs_set_kernel(int kernel) { g_kernel = kernel == 1 ? 1 : 0; }
+
+/* ZETASIG: Gaussian (gaussian.h:20-23) exp(-rb^2/2) / (sigma^3 (2 pi)^(3/2));
+ * high-order (highorder.h:20-24) 15 / (8 pi sigma^3 (rb^2 + 1)^(7/2)). */
+static inline double zeta_sig(double rho, double sigma) {
   const double rb = rho / sigma;
   const double s3 = sigma * sigma * sigma;
-  const double z = exp(-0.5 * rb * rb) / s3 / pow(2.0 * M_PI, 1.5);
-  const double phi = 0.25 / M_PI * erf(rb / sqrt(2.0)) / s3;
-  const double qq = (phi / rb - z) / (rb * rb);
+  if (g_kernel == 1) return 1.875 / M_PI / pow(rb * rb + 1.0, 3.5) / s3;
+  return exp(-0.5 * rb * rb) / s3 / pow(2.0 * M_PI, 1.5);
+}
+
+/* KERNEL, rb = rho/sigma.  Gaussian (gaussian.h:47-60):
+ *   phi  = erf(rb / sqrt 2) / (4 pi sigma^3)
+ *   q    = (phi/rb - zeta) / rb^2,  eta = zeta.
+ * High-order (highorder.h:31-61):
+ *   q    = rb^3 (rb^2 + 5/2) / (4 pi (rb^2 + 1)^(5/2) rho^3)
+ *   eta  = 105 / (8 pi sigma^3 (rb^2 + 1)^(9/2)).
+ * Both: F = (zeta - 3 q) / rho^2; eta is the diffusion kernel. */
+static inline void kernel_terms(double rho, double sigma, double *q, double *F, double *Z, double *eta) {
+  const double rb = rho / sigma;
+  const double s3 = sigma * sigma * sigma;
+  const double z = zeta_sig(rho, sigma);
+  double qq, n;
+  if (g_kernel == 1) {
+    const double w = rb * rb + 1.0;
+    qq = 0.25 / M_PI * rb * rb * rb * (rb * rb + 2.5) / pow(w, 2.5) / (rho * rho * rho);
+    n = 13.125 / M_PI / pow(w, 4.5) / s3;
+  } else {
+    const double phi = 0.25 / M_PI * erf(rb / sqrt(2.0)) / s3;
+    qq = (phi / rb - z) / (rb * rb);
+    n = z;
+  }
   *q = qq;
   *Z = z;
+  *eta = n;
   *F = (z - 3.0 * qq) / (rho * rho);
+}
+
+/* Enstrophy pair factors ENST / ENSTF (highorder.h:71-95; zero for the
+ * Gaussian kernel, gaussian.h:69-81), s2 = sigma^2, R = rho^2 + s2:
+ *   F1  = (2 rho^4 + 7 s2 rho^2 + 20 s2^2) / (8 pi R^(7/2))
+ *   F2  = -(6 rho^4 + 27 s2 rho^2 + 21 s2^2) / (8 pi R^(9/2))
+ *   F1F = 15 s2^2 / (8 pi R^(7/2)) */
+static inline void enst_terms(double r2, double s2, double *F1, double *F2, double *F1F) {
+  if (g_kernel != 1) { *F1 = *F2 = *F1F = 0.0; return; }
+  const double R = r2 + s2;
+  const double f = 0.125 / M_PI / sqrt(pow(R, 7.0));
+  *F1 = f * (2.0 * r2 * r2 + 7.0 * s2 * r2 + 20.0 * s2 * s2);
+  *F2 = f * (-6.0 * r2 * r2 - 27.0 * s2 * r2 - 21.0 * s2 * s2) / R;
+  *F1F = f * 15.0 * s2 * s2;
 }
 
 static inline void cross3(const double *a, const double *b, double *c) {
@@ -48,7 +86,7 @@ static inline void cross3(const double *a, const double *b, double *c) {
  * (interaction_utils.h:547):
  *   velocity   u_t  += q (alpha_s x d)                 (VELOCITY :55-62)
  *   stretching da_t += q (a_t x a_s) + F [d.(a_t x a_s)] d   (VORSTRETCH :73-105)
- *   diffusion  da_t += nu zeta / (sigma^2/2) (vol_t a_s - vol_s a_t)  (DIFFUSION :344-378)
+ *   diffusion  da_t += nu eta / (sigma^2/2) (vol_t a_s - vol_s a_t)  (DIFFUSION :344-378)
  * The source side of PAWAN's symmetric update (-q(a_t x d), -da) is the same
  * expression with the roles swapped (INTERACT :523-576). */
 static void rates_one(int64_t t, int64_t n, const double *pos, const double *alpha,
@@ -62,15 +100,15 @@ static void rates_one(int64_t t, int64_t n, const double *pos, const double *alp
     const double d[3] = {xt[0] - xs[0], xt[1] - xs[1], xt[2] - xs[2]};
     const double rho = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
     const double sg = sqrt(0.5 * (sigma[s] * sigma[s] + st * st));
-    double q, F, Z;
-    kernel_terms(rho, sg, &q, &F, &Z);
+    double q, F, Z, eta;
+    kernel_terms(rho, sg, &q, &F, &Z, &eta);
     double w[3];
     cross3(as, d, w);
     u0 += q * w[0]; u1 += q * w[1]; u2 += q * w[2];
     double c[3];
     cross3(at, as, c);
     const double dc = d[0] * c[0] + d[1] * c[1] + d[2] * c[2];
-    const double k = nu * Z / (0.5 * sg * sg);
+    const double k = nu * eta / (0.5 * sg * sg);
     const double vs = vol[s];
     d0 += q * c[0] + F * dc * d[0] + k * (vt * as[0] - vs * at[0]);
     d1 += q * c[1] + F * dc * d[1] + k * (vt * as[1] - vs * at[1]);
@@ -148,7 +186,12 @@ void rs_step(int scheme, double dt, int nsteps, int64_t n, double *pos, double *
  *   linear impulse   1/2 sum x x alpha
  *   angular impulse  1/3 sum x x (x x alpha)
  *   helicity         sum_{i != j} q(rho, s_ij) (x_j - x_i).(a_i x a_j)
- *   enstrophy[F]     0 for the Gaussian kernel (gaussian.h:69-92)
+ *   enstrophy        sum_i ENST(s_i) |a_i|^2
+ *                    + sum_{i != j} [F1 (a_i.a_j) + F2 (a_i.d)(a_j.d)]   (ENSTROPHY :107-176)
+ *   enstrophyF       sum_i ENSTF(s_i) |a_i|^2 + sum_{i != j} F1F (a_i.a_j)  (:122-201)
+ *                    with ENST(s) = 5/(2 pi s^3), ENSTF(s) = 15/(8 pi s^3)
+ *                    (highorder.h:101-110); both 0 for the Gaussian kernel
+ *                    (gaussian.h:69-92)
  *   KE   = sum_i |a_i|^2/(8 pi s_i)
  *        + sum_{i != j} [(rho^2 + 2 s^2)(a_i.a_j) + (d.a_i)(d.a_j)] / (16 pi (rho^2 + s^2)^(3/2))
  *   KEF  = sum_i 3|a_i|^2/(16 pi s_i)
@@ -166,21 +209,26 @@ void rs_diagnose(int nw, const int64_t *offsets, const double *pos, const double
     cross3(x, xa, xxa);
     for (int k = 0; k < 3; ++k) { O[k] += a[k]; I[k] += xa[k]; A[k] += xxa[k]; }
   }
-  double H = 0, KE = 0, KEF = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : H, KE, KEF)
+  double H = 0, KE = 0, KEF = 0, EN = 0, ENF = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : H, KE, KEF, EN, ENF)
   for (int64_t i = 0; i < n; ++i) {
     const double *xi = pos + 3 * i, *ai = alpha + 3 * i;
     const double si = sigma[i];
     const double a2 = ai[0] * ai[0] + ai[1] * ai[1] + ai[2] * ai[2];
     double h = 0, ke = a2 / si / 8.0 / M_PI, kef = 3.0 * a2 / (si * 16.0) / M_PI;
+    double en = 0, enf = 0;
+    if (g_kernel == 1) {
+      en = 5.0 / M_PI / 2.0 / (si * si * si) * a2;
+      enf = 15.0 / M_PI / 8.0 / (si * si * si) * a2;
+    }
     for (int64_t j = 0; j < n; ++j) {
       if (j == i) continue;
       const double *xj = pos + 3 * j, *aj = alpha + 3 * j;
       const double d[3] = {xj[0] - xi[0], xj[1] - xi[1], xj[2] - xi[2]};
       const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
       const double s2 = 0.5 * (si * si + sigma[j] * sigma[j]);
-      double q, F, Z;
-      kernel_terms(sqrt(r2), sqrt(s2), &q, &F, &Z);
+      double q, F, Z, eta;
+      kernel_terms(sqrt(r2), sqrt(s2), &q, &F, &Z, &eta);
       double c[3];
       cross3(ai, aj, c);
       h += q * (d[0] * c[0] + d[1] * c[1] + d[2] * c[2]);
@@ -190,8 +238,12 @@ void rs_diagnose(int nw, const int64_t *offsets, const double *pos, const double
       const double den = pow(r2 + s2, 1.5);
       ke += ((r2 + 2.0 * s2) * aa + dai * daj) / den / 16.0 / M_PI;
       kef += (r2 + 1.5 * s2) * aa / den / 8.0 / M_PI;
+      double F1, F2, F1F;
+      enst_terms(r2, s2, &F1, &F2, &F1F);
+      en += F1 * aa + F2 * dai * daj;
+      enf += F1F * aa;
     }
-    H += h; KE += ke; KEF += kef;
+    H += h; KE += ke; KEF += kef; EN += en; ENF += enf;
   }
   double zc = zc_prev;
   for (int w = 0; w < nw; ++w) {
@@ -206,7 +258,7 @@ void rs_diagnose(int nw, const int64_t *offsets, const double *pos, const double
     if (den != 0.0) zc = num / den;
   }
   for (int k = 0; k < 3; ++k) { out[k] = O[k]; out[3 + k] = 0.5 * I[k]; out[6 + k] = A[k] / 3.0; }
-  out[9] = H; out[10] = 0.0; out[11] = 0.0; out[12] = KE; out[13] = KEF; out[14] = zc;
+  out[9] = H; out[10] = EN; out[11] = ENF; out[12] = KE; out[13] = KEF; out[14] = zc;
   const double origin[3] = {0, 0, 0};
   rs_getvi(n, pos, alpha, sigma, origin, vbi);
 }
@@ -219,8 +271,8 @@ void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *s
   for (int64_t i = 0; i < n; ++i) {
     const double d[3] = {r[0] - pos[3 * i], r[1] - pos[3 * i + 1], r[2] - pos[3 * i + 2]};
     const double rho = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    double q, F, Z, w[3];
-    kernel_terms(rho, sigma[i], &q, &F, &Z);
+    double q, F, Z, eta, w[3];
+    kernel_terms(rho, sigma[i], &q, &F, &Z, &eta);
     cross3(alpha + 3 * i, d, w);
     for (int k = 0; k < 3; ++k) u[k] += q * w[k];
   }
@@ -231,8 +283,8 @@ void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *s
  * (interaction.cpp:212-260; INFLUENCE / SELFINFLUENCE, interaction_utils.h:
  * 626-703): k_t = sum_s ZETASIG(rho_ts, sigma_ts) alpha_s over every particle
  * s, the target itself included (rho = 0, sigma_tt = sigma_t), with
- * sigma_ts = sqrt((sigma_t^2 + sigma_s^2) / 2) and ZETASIG (gaussian.h:20-23)
- * = exp(-rho^2 / (2 sigma^2)) / sigma^3 / (2 pi)^1.5. */
+ * sigma_ts = sqrt((sigma_t^2 + sigma_s^2) / 2) and ZETASIG of the selected
+ * kernel (zeta_sig above). */
 void rs_vorticity_field(int64_t n, const double *pos, const double *alpha, const double *sigma,
                         const int64_t *targets, int64_t nt, double *field) {
   if (!targets) nt = n;
@@ -244,8 +296,7 @@ void rs_vorticity_field(int64_t n, const double *pos, const double *alpha, const
       const double dx = pos[3 * t] - pos[3 * s], dy = pos[3 * t + 1] - pos[3 * s + 1], dz = pos[3 * t + 2] - pos[3 * s + 2];
       const double rho = sqrt(dx * dx + dy * dy + dz * dz);
       const double sg = sqrt(0.5 * (sigma[t] * sigma[t] + sigma[s] * sigma[s]));
-      const double rb = rho / sg;
-      const double z = exp(-0.5 * rb * rb) / pow(sg, 3.0) / pow(2.0 * M_PI, 1.5);
+      const double z = zeta_sig(rho, sg);
       for (int m = 0; m < 3; ++m) k[m] += z * alpha[3 * s + m];
     }
     for (int m = 0; m < 3; ++m) field[3 * i + m] = k[m];

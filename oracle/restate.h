@@ -18,6 +18,11 @@
 extern "C" {
 #endif
 
+/* Selects the regularisation kernel of every later call: 0 = Gaussian
+ * (src/interaction/gaussian.h, the default), 1 = high-order algebraic
+ * (src/interaction/highorder.h).  Process-wide; not for concurrent callers. */
+void rs_set_kernel(int kernel);
+
 /* Rates dx/dt (vel) and dalpha/dt (dalpha) of the targets listed in
  * `targets` (nt entries; NULL means all n particles in order) induced by all n
  * particles, self excluded.  Outputs are (nt, 3) row-major. */

@@ -22,6 +22,10 @@ PGPU_ENUMERIC = -5
 
 FP32C = 0
 FP64 = 1
+# Regularisation kernels (PGPU_KERNEL_*): PAWAN's gaussian.h and highorder.h.
+GAUSSIAN = 0
+HIGHORDER = 1
+KERNELS = {"gaussian": GAUSSIAN, "highorder": HIGHORDER}
 EULER, RK3, RK4 = 0, 1, 2
 SCHEMES = {"euler": EULER, "rk3": RK3, "rk4": RK4}
 
@@ -44,7 +48,8 @@ EXPORTS = [
 
 class PgpuConfig(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("nu", C.c_double), ("vinf", C.c_double * 3),
-                ("block", C.c_int), ("tpt", C.c_int), ("chunks", C.c_int), ("use_graphs", C.c_int)]
+                ("block", C.c_int), ("tpt", C.c_int), ("chunks", C.c_int), ("use_graphs", C.c_int),
+                ("kernel", C.c_int)]
 
 
 class SurrogateConfig(C.Structure):
@@ -213,7 +218,7 @@ class Context:
     """One backend context: wakes grouped into systems, all device-resident."""
 
     def __init__(self, precision: int = FP32C, nu: float = 1.56e-5, device: int = 0, vinf=(0.0, 0.0, 0.0),
-                 block: int = 0, tpt: int = 0, chunks: int = 0, use_graphs: bool = True):
+                 block: int = 0, tpt: int = 0, chunks: int = 0, use_graphs: bool = True, kernel: int = GAUSSIAN):
         self.lib = load()
         cfg = PgpuConfig()
         self.lib.pgpu_config_default(C.byref(cfg))
@@ -224,6 +229,7 @@ class Context:
             cfg.vinf[k] = float(vinf[k])
         cfg.block, cfg.tpt, cfg.chunks = block, tpt, chunks
         cfg.use_graphs = 1 if use_graphs else 0
+        cfg.kernel = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
         h = C.c_void_p()
         rc = self.lib.pgpu_create(C.byref(h), C.byref(cfg))
         if rc != PGPU_OK:

@@ -33,7 +33,7 @@ constexpr int kMaxChunks = 16;
 // Sources per compensation group of the FP32 pair kernel: plain FP32 partial
 // sums over this many sources, then one error-free two-sum per component.
 constexpr int kPairCG = 64;
-constexpr int kDiagFields = 19;
+constexpr int kDiagFields = 23;
 // FP64 far regime: u = rho^2 / sigma^2 >= 100, where erfc(sqrt(u/2)) and the
 // e^{-u/2} terms of q and F vanish at double precision (the closed form and
 // the far limit agree to the last bit from u ~ 90 on).
@@ -174,10 +174,20 @@ __device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s) {
 // (TILE == BLOCK: each thread stages one record), CG sources per compensation
 // group (plain FP32 partial sums over CG sources, then an error-free two-sum
 // into the per-target (hi, lo) accumulators).
-// This generic body serves the FP64 mode; the FP32 mode uses
+// This generic body serves the FP64 mode of the Gaussian kernel and both modes
+// of the high-order kernel (KER = kHighOrder: every pair takes pair_terms_ho,
+// which has no far regime to skip); the FP32 Gaussian mode uses
 // pair_body_f32 (pair_f32.cuh), the same decomposition with packed FP32.
-template <typename T, int BLOCK, int TPT, int CG>
+template <typename T, int BLOCK, int TPT, int CG, int KER>
 __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
+  constexpr bool kGauss32 = sizeof(T) == 4 && KER == kGaussian;
+  // Stretching q (a_t x a_s): summed as alpha_t x (sum q alpha_s) per
+  // compensation group, except for the FP32 high-order kernel, which forms
+  // a_t x a_s per pair.  Along a vortex tube a_t and the group sum are nearly
+  // parallel, so the cross product of the sum cancels and keeps the sum's
+  // FP32 rounding; the high-order q is ~9x larger than the Gaussian one near
+  // rho = 0, which lifts that error to ~1e-5 of max |dalpha| on a ring.
+  constexpr bool kPairCross = sizeof(T) == 4 && KER == kHighOrder;
   constexpr int TILE = BLOCK;
   constexpr int TT = BLOCK * TPT;
   static_assert(TILE % CG == 0, "compensation group must divide the tile");
@@ -224,7 +234,7 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
     // FP32: bounding box of this warp's targets and their largest sigma^2/2,
     // for the per-tile all-far test below
     WarpBox tb;
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (kGauss32) {
       tb.init();
 #pragma unroll
       for (int k = 0; k < TPT; ++k) tb.add(xt[k][0], xt[k][1], xt[k][2], hst[k]);
@@ -258,7 +268,7 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
       // is never misclassified near; a pair within rounding of u = 50 may take
       // the far limit, whose dropped terms are below 2e-9 there.
       bool far_tile = false;
-      if constexpr (sizeof(T) == 4) {
+      if constexpr (kGauss32) {
         WarpBox sb_box;
         sb_box.init();
         for (int r = lane; r < TILE; r += 32) {
@@ -309,7 +319,13 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
             const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
             const T r2 = dx * dx + dy * dy + dz * dz;
             T qq, FF;
-            if constexpr (sizeof(T) == 4) {
+            if constexpr (KER == kHighOrder) {
+              const PairTerms<T> pt = pair_terms_ho(r2, hst[k] + p.w);
+              qq = pt.q; FF = pt.F;
+              sdv[k][0] += pt.zd * (vt[k] * q.x - q.w * at[k][0]);
+              sdv[k][1] += pt.zd * (vt[k] * q.y - q.w * at[k][1]);
+              sdv[k][2] += pt.zd * (vt[k] * q.z - q.w * at[k][2]);
+            } else if constexpr (sizeof(T) == 4) {
               // far test r^2 >= 50 (hs_t + hs_s) as one FMA against the
               // target's precomputed 50 hs_t
               const bool near = fmaf(-kFarU, p.w, r2) < h50[k];
@@ -360,16 +376,31 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
             // d . (alpha_t x alpha_s) = alpha_t . w
             const T fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
             sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
-            sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
+            if constexpr (kPairCross) {
+              // sp holds sum q (alpha_t x alpha_s) itself
+              sp[k][0] += qq * (at[k][1] * q.z - at[k][2] * q.y);
+              sp[k][1] += qq * (at[k][2] * q.x - at[k][0] * q.z);
+              sp[k][2] += qq * (at[k][0] * q.y - at[k][1] * q.x);
+            } else {
+              sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
+            }
           }
         }
         }
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
           // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t)
-          const T ex = at[k][1] * sp[k][2] - at[k][2] * sp[k][1] + sd[k][0] + a.nu2 * sdv[k][0];
-          const T ey = at[k][2] * sp[k][0] - at[k][0] * sp[k][2] + sd[k][1] + a.nu2 * sdv[k][1];
-          const T ez = at[k][0] * sp[k][1] - at[k][1] * sp[k][0] + sd[k][2] + a.nu2 * sdv[k][2];
+          T cx, cy, cz;
+          if constexpr (kPairCross) {
+            cx = sp[k][0]; cy = sp[k][1]; cz = sp[k][2];
+          } else {
+            cx = at[k][1] * sp[k][2] - at[k][2] * sp[k][1];
+            cy = at[k][2] * sp[k][0] - at[k][0] * sp[k][2];
+            cz = at[k][0] * sp[k][1] - at[k][1] * sp[k][0];
+          }
+          const T ex = cx + sd[k][0] + a.nu2 * sdv[k][0];
+          const T ey = cy + sd[k][1] + a.nu2 * sdv[k][1];
+          const T ez = cz + sd[k][2] + a.nu2 * sdv[k][2];
           two_sum_acc(vh[k][0], vl[k][0], sv[k][0]);
           two_sum_acc(vh[k][1], vl[k][1], sv[k][1]);
           two_sum_acc(vh[k][2], vl[k][2], sv[k][2]);
@@ -382,7 +413,7 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
       buf ^= 1;
     }
     cp_async_wait<0>();
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (kGauss32) {
       const unsigned wsum = __reduce_add_sync(0xffffffffu, nfull);
       if ((tid & 31) == 0 && wsum) atomicAdd(a.nfull, (unsigned long long)wsum);
       nfull = 0;
@@ -409,13 +440,15 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
 
 namespace pgpu {
 
-template <typename T, int BLOCK, int TPT>
-constexpr int pair_min_blocks() { return sizeof(T) == 4 ? pair_f32_min_blocks<BLOCK, TPT>() : 1; }
+template <typename T, int BLOCK, int TPT, int KER>
+constexpr int pair_min_blocks() {
+  return sizeof(T) == 4 && KER == kGaussian ? pair_f32_min_blocks<BLOCK, TPT>() : 1;
+}
 
-template <typename T, int BLOCK, int TPT, int CG>
-__global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT>())) pair_kernel(PairArgs<T> a) {
-  if constexpr (sizeof(T) == 4) pair_body_f32<BLOCK, TPT, CG>(a);
-  else pair_body_generic<T, BLOCK, TPT, CG>(a);
+template <typename T, int BLOCK, int TPT, int CG, int KER = kGaussian>
+__global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT, KER>())) pair_kernel(PairArgs<T> a) {
+  if constexpr (sizeof(T) == 4 && KER == kGaussian) pair_body_f32<BLOCK, TPT, CG>(a);
+  else pair_body_generic<T, BLOCK, TPT, CG, KER>(a);
 }
 
 // ---------------------------------------------------------------- stage kernel
@@ -565,7 +598,7 @@ static __global__ void flat_kernel(double *flat, int64_t n, int64_t maxn, int64_
 template <typename T> struct DiagArgs {
   const v4_t<T> *P;
   const v4_t<T> *Q;
-  double *partial;  // [nch][6][cap]: components 0..2 = helicity, KE, KEF row sums
+  double *partial;  // [nch][6][cap]: components 0..4 = helicity, KE, KEF, enstrophy, enstrophyF row sums
   const PlanEntry *plan;
   int nsys;
   int nch;
@@ -577,13 +610,19 @@ template <typename T> struct DiagArgs {
 //   helicity  q(rho, s_ts) (x_s - x_t).(a_t x a_s)            (HELICITY, interaction_utils.h:214-242)
 //   KE        [(rho^2 + 2 s^2) a_t.a_s + (d.a_t)(d.a_s)] / (16 pi (rho^2 + s^2)^1.5)   (:278-306)
 //   KEF       (rho^2 + 1.5 s^2) a_t.a_s / (8 pi (rho^2 + s^2)^1.5)                    (:308-331)
-// All three terms are symmetric in (t, s), so each unordered pair is
+// and, for the high-order kernel only (the Gaussian ENST / ENSTF are zero,
+// gaussian.h:69-92), with R = rho^2 + s^2 (ENSTROPHY[F], interaction_utils.h:
+// 141-201; ENST / ENSTF, highorder.h:71-95):
+//   enstrophy  [(2 rho^4 + 7 s^2 rho^2 + 20 s^4) a_t.a_s
+//               - (6 rho^4 + 27 s^2 rho^2 + 21 s^4) (d.a_t)(d.a_s) / R] / (8 pi R^3.5)
+//   enstrophyF 15 s^4 a_t.a_s / (8 pi R^3.5)
+// All terms are symmetric in (t, s), so each unordered pair is
 // evaluated once, from its lower index (sources s > t only), and the row sums
 // are doubled: they then equal sums over ordered pairs, PAWAN's 2 x sum over
-// unordered pairs.  In FP32 the helicity's q takes the far limit 1/rho^3 for
-// u >= 50 (as in the rate kernel) and the mid/series terms only when some lane
-// of the warp needs them.
-template <typename T, int BLOCK>
+// unordered pairs.  In FP32 the Gaussian helicity's q takes the far limit
+// 1/rho^3 for u >= 50 (as in the rate kernel) and the mid/series terms only
+// when some lane of the warp needs them.
+template <typename T, int BLOCK, int KER = kGaussian>
 __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
   __shared__ __align__(16) v4_t<T> sP[BLOCK];
   __shared__ __align__(16) v4_t<T> sQ[BLOCK];
@@ -607,14 +646,14 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
     const int64_t s1 = min(pe.off + (int64_t)c * pe.chunk + pe.chunk, tend);
     const v4_t<T> pt = a.P[t], qt = a.Q[t];
     const T h50 = T(kFarU) * pt.w;
-    double h = 0, ke = 0, kef = 0;
+    double h = 0, ke = 0, kef = 0, en = 0, enf = 0;
     for (int64_t sb = s0; sb < s1; sb += BLOCK) {
       __syncthreads();
       const int64_t j = sb + tid;
       if (j < s1) { sP[tid] = a.P[j]; sQ[tid] = a.Q[j]; }
       else { sP[tid] = pad_P<T>(); sQ[tid] = pad_Q<T>(); }
       __syncthreads();
-      T hh = 0, kk = 0, kf = 0;
+      T hh = 0, kk = 0, kf = 0, ee = 0, ef = 0;
       const int cnt = (int)min((int64_t)BLOCK, s1 - sb);
       const bool diag = sb <= tlo + BLOCK - 1;  // the tile may still see s <= t
       for (int jj = 0; jj < cnt; ++jj) {
@@ -624,7 +663,9 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
         const T r2 = dx * dx + dy * dy + dz * dz;
         const T s2 = pt.w + p.w;
         T kq;
-        if constexpr (sizeof(T) == 4) {
+        if constexpr (KER == kHighOrder) {
+          kq = pair_terms_ho(r2, s2).q;
+        } else if constexpr (sizeof(T) == 4) {
           const bool near = fmaf(-kFarU, p.w, r2) < h50;
           const float ir = fast_rsqrt(r2);
           kq = ir * ir * ir;
@@ -645,17 +686,29 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
         const T das = dx * q.x + dy * q.y + dz * q.z;
         const T rs = r2 + s2;
         T ir;
-        if constexpr (sizeof(T) == 4) ir = fast_rsqrt(rs); else ir = rsqrt(rs);
+        // the enstrophy terms carry R^-4.5: a refined root keeps their FP32 error at rounding level
+        if constexpr (sizeof(T) == 4) ir = KER == kHighOrder ? rsqrt_nr(rs) : fast_rsqrt(rs);
+        else ir = rsqrt(rs);
         const T ir3 = ir * ir * ir;
         if (use) {
           hh -= kq * (dx * cx + dy * cy + dz * cz);
           kk += ((r2 + T(2) * s2) * aa + dat * das) * ir3;
           kf += (r2 + T(1.5) * s2) * aa * ir3;
+          if constexpr (KER == kHighOrder) {
+            const T ir7 = ir3 * ir3 * ir;
+            const T r4 = r2 * r2, s4 = s2 * s2, rs2 = r2 * s2;
+            const T f1 = T(2) * r4 + T(7) * rs2 + T(20) * s4;
+            const T f2 = T(6) * r4 + T(27) * rs2 + T(21) * s4;
+            ee += (f1 * aa - f2 * (ir * ir) * (dat * das)) * ir7;
+            ef += s4 * aa * ir7;
+          }
         }
       }
       h += (double)hh;
       ke += (double)kk;
       kef += (double)kf;
+      en += (double)ee;
+      enf += (double)ef;
     }
     if (valid) {
       // doubled: each unordered pair was summed once
@@ -663,6 +716,10 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
       o[0] = h * (2.0 * kInv4Pi);
       o[a.cap] = ke * (2.0 * kInv4Pi * 0.25);      // 1/(16 pi)
       o[2 * a.cap] = kef * (2.0 * kInv4Pi * 0.5);  // 1/(8 pi)
+      if constexpr (KER == kHighOrder) {
+        o[3 * a.cap] = en * (2.0 * kInv4Pi * 0.5);          // 1/(8 pi)
+        o[4 * a.cap] = enf * (2.0 * kInv4Pi * 0.5 * 15.0);  // 15/(8 pi)
+      }
     }
   }
 }
@@ -678,7 +735,9 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
 // rounding into percent-level strength errors.  Per target and source chunk,
 // row sums go to partial[c][0..2][t]; field_reduce_kernel adds the chunks.
 // A warp whose pairs all have u > 1500 skips the exponential: e^{-750} is
-// below the smallest double, so the term is exactly zero anyway.
+// below the smallest double, so the term is exactly zero anyway.  The
+// high-order kernel (KER = kHighOrder) takes its own ZETASIG (highorder.h:
+// 20-24), zeta = 1.875 / (pi sigma^3 (rho^2/sigma^2 + 1)^3.5), for every pair.
 struct FieldArgs {
   const double *x0;   // [6][cap] state
   const double *sig;  // [cap]
@@ -690,7 +749,7 @@ struct FieldArgs {
   unsigned int *counters;
 };
 
-template <int BLOCK>
+template <int BLOCK, int KER = kGaussian>
 __global__ void __launch_bounds__(BLOCK) field_kernel(FieldArgs a) {
   __shared__ __align__(16) double4 sP[BLOCK];  // (x, y, z, sigma^2 / 2)
   __shared__ __align__(16) double4 sQ[BLOCK];  // (alpha, 0)
@@ -732,8 +791,15 @@ __global__ void __launch_bounds__(BLOCK) field_kernel(FieldArgs a) {
         const double r2 = dx * dx + dy * dy + dz * dz;
         const double s2 = hst + p.w;
         double z = 0.0;
-        const bool live = r2 < 1500.0 * s2;
-        if (__any_sync(0xffffffffu, live)) z = kInv2Pi15 / (s2 * sqrt(s2)) * exp(-0.5 * r2 / s2);
+        if constexpr (KER == kHighOrder) {
+          const double is = 1.0 / sqrt(s2);
+          const double iw = 1.0 / sqrt(r2 / s2 + 1.0);
+          const double iw2 = iw * iw;
+          z = (HighOrder::kZeta * kInv4Pi) * (is * is * is) * (iw2 * iw2 * iw2 * iw);
+        } else {
+          const bool live = r2 < 1500.0 * s2;
+          if (__any_sync(0xffffffffu, live)) z = kInv2Pi15 / (s2 * sqrt(s2)) * exp(-0.5 * r2 / s2);
+        }
         k[0] += z * q.x;
         k[1] += z * q.y;
         k[2] += z * q.z;
@@ -765,7 +831,11 @@ static __global__ void field_reduce_kernel(const double *partial, int nch, int64
 // Fields (per CTA partial, summed on the host in CTA order):
 //   0-2 sum alpha, 3-5 sum x x alpha, 6-8 sum x x (x x alpha), 9 Zc numerator,
 //   10 Zc denominator, 11-13 velocity at the origin (getVi), 14 helicity,
-//   15 KE pair sum, 16 KEF pair sum, 17 KE self terms, 18 KEF self terms.
+//   15 KE pair sum, 16 KEF pair sum, 17 KE self terms, 18 KEF self terms,
+//   19 enstrophy pair sum, 20 enstrophyF pair sum, 21 enstrophy self terms
+//   5 |a|^2 / (2 pi s^3), 22 enstrophyF self terms 15 |a|^2 / (8 pi s^3)
+//   (ENST(sigma) / ENSTF(sigma), highorder.h:101-110; 19-22 stay zero for the
+//   Gaussian kernel, whose ENST / ENSTF are zero).
 __device__ __forceinline__ double block_sum(double v, double *red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -779,7 +849,7 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 static __global__ void diag_wake_kernel(const double *x0, const double *sig, const double *partial, int nch, int64_t cap,
-                                 int64_t lo, int64_t hi, int quad, double *out) {
+                                 int64_t lo, int64_t hi, int quad, int ker, double *out) {
   __shared__ double red[32];
   double f[kDiagFields];
 #pragma unroll
@@ -798,8 +868,7 @@ static __global__ void diag_wake_kernel(const double *x0, const double *sig, con
     // getVi at the origin with the particle's own radius: d = -x
     const double s = sig[i];
     const double r2 = rr + z * z;
-    const PairTerms<double> k = pair_terms(r2, s * s);
-    const double q = k.q * kInv4Pi;
+    const double q = (ker == kHighOrder ? pair_terms_ho(r2, s * s).q : pair_terms(r2, s * s).q) * kInv4Pi;
     f[11] += q * (ay * (-z) - az * (-y));
     f[12] += q * (az * (-x) - ax * (-z));
     f[13] += q * (ax * (-y) - ay * (-x));
@@ -811,10 +880,23 @@ static __global__ void diag_wake_kernel(const double *x0, const double *sig, con
         kef += partial[((int64_t)c * 6 + 2) * cap + i];
       }
       f[14] += h; f[15] += ke; f[16] += kef;
+      if (ker == kHighOrder) {
+        double en = 0, enf = 0;
+        for (int c = 0; c < nch; ++c) {
+          en += partial[((int64_t)c * 6 + 3) * cap + i];
+          enf += partial[((int64_t)c * 6 + 4) * cap + i];
+        }
+        f[19] += en; f[20] += enf;
+      }
     }
     const double a2 = ax * ax + ay * ay + az * az;
     f[17] += a2 / s * (kInv4Pi * 0.5);    // |a|^2 / (8 pi s)
     f[18] += a2 / s * (kInv4Pi * 0.75);   // 3 |a|^2 / (16 pi s)
+    if (ker == kHighOrder) {
+      const double is3 = 1.0 / (s * s * s);
+      f[21] += a2 * is3 * (kInv4Pi * 10.0);  // 5 |a|^2 / (2 pi s^3)
+      f[22] += a2 * is3 * (kInv4Pi * 7.5);   // 15 |a|^2 / (8 pi s^3)
+    }
   }
   for (int m = 0; m < kDiagFields; ++m) {
     const double r = block_sum(f[m], red);
@@ -824,8 +906,9 @@ static __global__ void diag_wake_kernel(const double *x0, const double *sig, con
 
 // Velocity induced at arbitrary points by particles [lo, hi) with each
 // particle's own radius (PAWAN __interaction::getVi, interaction.cpp:453-477;
-// the blade-airstation inflow of getInflow, :399-451).
-template <int BLOCK>
+// the blade-airstation inflow of getInflow, :399-451), with the q of the
+// selected kernel (KER).
+template <int BLOCK, int KER = kGaussian>
 __global__ void __launch_bounds__(BLOCK) probe_kernel(const double *x0, const double *sig, int64_t cap, int64_t lo,
                                                       int64_t hi, const double *pts, int64_t npts, double *vel) {
   __shared__ double sx[BLOCK][7];
@@ -846,8 +929,8 @@ __global__ void __launch_bounds__(BLOCK) probe_kernel(const double *x0, const do
     for (int jj = 0; jj < cnt; ++jj) {
       const double dx = rx - sx[jj][0], dy = ry - sx[jj][1], dz = rz - sx[jj][2];
       const double s = sx[jj][6];
-      const PairTerms<double> k = pair_terms(dx * dx + dy * dy + dz * dz, s * s);
-      const double q = k.q * kInv4Pi;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double q = (KER == kHighOrder ? pair_terms_ho(r2, s * s).q : pair_terms(r2, s * s).q) * kInv4Pi;
       const double ax = sx[jj][3], ay = sx[jj][4], az = sx[jj][5];
       u0 += q * (ay * dz - az * dy);
       u1 += q * (az * dx - ax * dz);

@@ -45,15 +45,19 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 template <typename T> using PairFn = void (*)(PairArgs<T>);
 
-template <typename T> PairFn<T> pair_fn(int s) {
+template <typename T, int KER> PairFn<T> pair_fn_k(int s) {
   switch (s) {
-    case 0: return pair_kernel<T, 128, 1, kCG>;
-    case 1: return pair_kernel<T, 128, 2, kCG>;
-    case 2: return pair_kernel<T, 256, 1, kCG>;
-    case 3: return pair_kernel<T, 256, 2, kCG>;
-    case 4: return pair_kernel<T, 64, 2, kCG>;
-    default: return pair_kernel<T, 128, 4, kCG>;
+    case 0: return pair_kernel<T, 128, 1, kCG, KER>;
+    case 1: return pair_kernel<T, 128, 2, kCG, KER>;
+    case 2: return pair_kernel<T, 256, 1, kCG, KER>;
+    case 3: return pair_kernel<T, 256, 2, kCG, KER>;
+    case 4: return pair_kernel<T, 64, 2, kCG, KER>;
+    default: return pair_kernel<T, 128, 4, kCG, KER>;
   }
+}
+// Pair kernel of shape s for regularisation kernel `ker` (PGPU_KERNEL_*).
+template <typename T> PairFn<T> pair_fn(int s, int ker) {
+  return ker == PGPU_KERNEL_HIGHORDER ? pair_fn_k<T, kHighOrder>(s) : pair_fn_k<T, kGaussian>(s);
 }
 
 struct WakeRec {
@@ -163,7 +167,7 @@ int check_contiguous(pgpu_ctx *c) {
 
 template <typename T> int occupancy(pgpu_ctx *c, int s) {
   int nb = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pair_fn<T>(s), kShapes[s].block, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pair_fn<T>(s, c->cfg.kernel), kShapes[s].block, 0);
   if (e != cudaSuccess || nb < 1) nb = 1;
   return nb * c->sms;
 }
@@ -347,7 +351,7 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   // the graph when it is marked external.
   const unsigned flags = c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][0], c->st, flags));
-  pair_fn<T>(c->shape)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
+  pair_fn<T>(c->shape, c->cfg.kernel)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
   CK(cudaGetLastError());
   if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][1], c->st, flags));
   c->launches++;
@@ -457,6 +461,10 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
   if (cfg) c->cfg = *cfg;
   else pgpu_config_default(&c->cfg);
   if (c->cfg.precision != PGPU_FP32C && c->cfg.precision != PGPU_FP64) {
+    delete c;
+    return PGPU_EINVAL;
+  }
+  if (c->cfg.kernel != PGPU_KERNEL_GAUSSIAN && c->cfg.kernel != PGPU_KERNEL_HIGHORDER) {
     delete c;
     return PGPU_EINVAL;
   }
@@ -736,16 +744,19 @@ int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
   const bool quad = plan.size() > 1;
   if (quad) {
     int grid = 0;
+    const bool ho = c->cfg.kernel == PGPU_KERNEL_HIGHORDER;
     if (fp64(c)) {
       DiagArgs<double> a{static_cast<const double4 *>(c->P), static_cast<const double4 *>(c->Q), c->partial,
                          c->d_plan_diag, 1, nch, c->cap, c->d_counters};
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, diag_pair_kernel<double, 256>, block, 0);
-      diag_pair_kernel<double, 256><<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
+      auto fn = ho ? diag_pair_kernel<double, 256, kHighOrder> : diag_pair_kernel<double, 256, kGaussian>;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, fn, block, 0);
+      fn<<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
     } else {
       DiagArgs<float> a{static_cast<const float4 *>(c->P), static_cast<const float4 *>(c->Q), c->partial,
                         c->d_plan_diag, 1, nch, c->cap, c->d_counters};
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, diag_pair_kernel<float, 256>, block, 0);
-      diag_pair_kernel<float, 256><<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
+      auto fn = ho ? diag_pair_kernel<float, 256, kHighOrder> : diag_pair_kernel<float, 256, kGaussian>;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, fn, block, 0);
+      fn<<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
     }
     CK(cudaGetLastError());
     c->launches++;
@@ -757,7 +768,8 @@ int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
     const WakeRec &W = c->wakes[w];
     if (W.n == 0) continue;
     const int grid = (int)std::min<int64_t>(ceil_div(W.n, 256), c->diag_blocks);
-    diag_wake_kernel<<<grid, 256, 0, c->st>>>(c->x0, c->sig, c->partial, nch, c->cap, W.off, W.off + W.n, quad ? 1 : 0, c->d_diag);
+    diag_wake_kernel<<<grid, 256, 0, c->st>>>(c->x0, c->sig, c->partial, nch, c->cap, W.off, W.off + W.n, quad ? 1 : 0,
+                                              c->cfg.kernel, c->d_diag);
     CK(cudaGetLastError());
     c->launches++;
     CK(cudaMemcpyAsync(h.data(), c->d_diag, (size_t)grid * kDiagFields * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -775,8 +787,8 @@ int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
     out[6 + m] = f[6 + m] / 3.0;
   }
   out[9] = f[14];
-  out[10] = 0.0;
-  out[11] = 0.0;
+  out[10] = f[21] + f[19];
+  out[11] = f[22] + f[20];
   out[12] = f[17] + f[15];
   out[13] = f[18] + f[16];
   out[14] = zc;
@@ -797,7 +809,8 @@ int pgpu_probe(pgpu_ctx *c, int32_t system, int64_t npts, const double *pts, dou
   CK(cudaMemsetAsync(d + 3 * npts, 0, 3 * npts * sizeof(double), c->st));
   const int64_t lo = c->sys[system].off, hi = lo + sys_n(c, system);
   if (hi > lo) {
-    probe_kernel<128><<<(unsigned)ceil_div(npts, 128), 128, 0, c->st>>>(c->x0, c->sig, c->cap, lo, hi, d, npts, d + 3 * npts);
+    auto fn = c->cfg.kernel == PGPU_KERNEL_HIGHORDER ? probe_kernel<128, kHighOrder> : probe_kernel<128, kGaussian>;
+    fn<<<(unsigned)ceil_div(npts, 128), 128, 0, c->st>>>(c->x0, c->sig, c->cap, lo, hi, d, npts, d + 3 * npts);
     CK(cudaGetLastError());
     c->launches++;
   }
@@ -851,8 +864,9 @@ int pgpu_influence(pgpu_ctx *c) {
   if (plan.size() > 1 && plan.front().n > 0) {
     int grid = 0;
     FieldArgs a{c->x0, c->sig, c->partial, c->d_plan_field, (int)c->sys.size(), nch, c->cap, c->d_counters};
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, field_kernel<256>, block, 0));
-    field_kernel<256><<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
+    auto fn = c->cfg.kernel == PGPU_KERNEL_HIGHORDER ? field_kernel<256, kHighOrder> : field_kernel<256, kGaussian>;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, fn, block, 0));
+    fn<<<std::max(1, grid) * c->sms, block, 0, c->st>>>(a);
     CK(cudaGetLastError());
     c->launches++;
   }
@@ -909,7 +923,8 @@ int64_t pgpu_launch_count(pgpu_ctx *c) { return c ? c->launches : -1; }
 int pgpu_pair_counts(pgpu_ctx *c, int64_t *pairs, int64_t *full_pairs) {
   if (!c) return PGPU_EINVAL;
   int64_t full = c->pairs_acc;
-  if (c->frozen && !fp64(c)) {
+  // only the FP32C Gaussian kernel has a far regime (and counts its full pairs)
+  if (c->frozen && !fp64(c) && c->cfg.kernel == PGPU_KERNEL_GAUSSIAN) {
     unsigned long long nf = 0;
     CK(cudaStreamSynchronize(c->st));
     CK(cudaMemcpy(&nf, c->d_nfull, sizeof(nf), cudaMemcpyDeviceToHost));

@@ -8,12 +8,14 @@ namespace pawan {
 
 __gpu::__gpu(__wake *W, const pgpu_config &cfg) : __interaction(), _cfg(cfg) {
   _nu = cfg.nu;  // the base constructor hard-codes 1.56e-5 (interaction.cpp:15)
+  _cfg.kernel = pawan_kernel();
   check(pgpu_create(&_ctx, &_cfg));
   addWake(W);
 }
 
 __gpu::__gpu(__wake *W1, __wake *W2, const pgpu_config &cfg) : __interaction(), _cfg(cfg) {
   _nu = cfg.nu;
+  _cfg.kernel = pawan_kernel();
   check(pgpu_create(&_ctx, &_cfg));
   addWake(W1);
   addWake(W2);

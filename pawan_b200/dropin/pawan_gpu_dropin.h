@@ -21,6 +21,10 @@
  * (one CUDA graph per step), and the state vector and the wakes are updated
  * afterwards, as PAWAN's step leaves them (rk4.cpp:66-68).
  *
+ * Kernel: __gpu always uses the regularisation kernel this PAWAN build was
+ * compiled with (pawan_kernel() below), whatever cfg.kernel says, so that it
+ * computes what the __interaction it replaces would.
+ *
  * Errors: a non-zero pgpu_* status becomes std::runtime_error carrying
  * pgpu_last_error().  A GPU integrator given a system that is not a __gpu
  * throws std::invalid_argument (there is no CPU fallback).
@@ -36,6 +40,17 @@
 #include "src/interaction/interaction.h"
 
 namespace pawan {
+
+// PGPU_KERNEL_* of the kernel compiled into this PAWAN build: HIGHORDER /
+// GAUSSIAN (interaction_utils.h:13-20) make interaction.h include either
+// highorder.h, which defines HIGHORDER_H_, or gaussian.h.
+inline int pawan_kernel() {
+#ifdef HIGHORDER_H_
+  return PGPU_KERNEL_HIGHORDER;
+#else
+  return PGPU_KERNEL_GAUSSIAN;
+#endif
+}
 
 class __gpu : public __interaction {
  public:

@@ -22,6 +22,14 @@ def ref_available():
 
 
 @pytest.fixture(scope="session")
+def ref_ho_available():
+    from oracle import oracle as O
+    if not O.ref_available("highorder"):
+        pytest.skip("oracle/_ref/libpawanref_ho.so is not built (make -C oracle)")
+    return True
+
+
+@pytest.fixture(scope="session")
 def gpu():
     import torch
     if not torch.cuda.is_available():

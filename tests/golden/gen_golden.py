@@ -1,10 +1,12 @@
 """Generates the golden fixtures under tests/golden/ from PAWAN's own code.
 
-    make -C oracle && python tests/golden/gen_golden.py
+    make -C oracle && python tests/golden/gen_golden.py [name ...]
 
 Every output comes from ``oracle/_ref/libpawanref.so``: PAWAN's unmodified
 interaction / parallel / integration / wake sources compiled against the
-project's GSL-subset shim (``oracle/Makefile``).  Inputs come from the seeded
+project's GSL-subset shim (``oracle/Makefile``); the ``*_ho`` fixtures come
+from ``oracle/_ref/libpawanref_ho.so``, the same sources built with PAWAN's
+high-order algebraic kernel (src/interaction/highorder.h).  Inputs come from the seeded
 generators in ``pawan_b200.cases``; their SHA-256 is stored so a test can
 check that regenerating the inputs reproduces the fixture's inputs.
 
@@ -18,6 +20,12 @@ Fixtures:
   twowake.npz    - two interacting wakes in one system (leapfrog pair, N=400+320).
   integrate/     - the .wake / .diagnosis files of PAWAN's own
                    __integration::integrate for 3 RK4 steps of ring1000.
+  ring1000_ho.npz - ring1000's inputs (checked by SHA-256) with the high-order
+                   kernel: rates, diagnostics (enstrophy and enstrophyF are
+                   non-zero for it) and vbi, the vorticity field of
+                   influence(), the state after 2 RK4 and after 2 RK3 steps.
+  twowake_ho.npz - twowake's inputs with the high-order kernel: rates of both
+                   wakes and the diagnostics (cross-wake enstrophy terms).
 """
 from __future__ import annotations
 
@@ -88,6 +96,35 @@ def twowake():
                         vel2=v2, dalpha2=d2, diag=diag, nu=NU)
 
 
+def ring1000_ho():
+    w = cases.ring_stations(stations=40, seed=0)
+    R = O.RefSystem([w], NU, kernel="highorder")
+    R.solve()
+    vel, da = R.rates()
+    diag = R.diagnose()
+    vbi = R.getvi([0.0, 0.0, 0.0])
+    field = R.vorticity_field()
+    R.step("rk4", 0.01, 2)
+    x4, a4 = R.state()
+    R3 = O.RefSystem([w], NU, kernel="highorder")
+    R3.step("rk3", 0.01, 2)
+    x3, a3 = R3.state()
+    np.savez_compressed(OUT / "ring1000_ho.npz", nu=NU, vel=vel, dalpha=da, diag=diag, vbi=vbi, field=field,
+                        rk4_pos=x4, rk4_alpha=a4, rk3_pos=x3, rk3_alpha=a3, dt=0.01, sha256=digest(w))
+
+
+def twowake_ho():
+    w1 = cases.ring_stations(stations=16, seed=3)
+    w2 = cases.ring_stations(R=1.2, stations=16, z0=0.3, seed=5).subset(320)
+    R = O.RefSystem([w1, w2], NU, kernel="highorder")
+    R.solve()
+    v1, d1 = R.rates(0)
+    v2, d2 = R.rates(1)
+    diag = R.diagnose()
+    np.savez_compressed(OUT / "twowake_ho.npz", vel1=v1, dalpha1=d1, vel2=v2, dalpha2=d2, diag=diag, nu=NU,
+                        sha256=digest(w1) + digest(w2))
+
+
 def integrate_files():
     d = OUT / "integrate"
     d.mkdir(exist_ok=True)
@@ -96,11 +133,12 @@ def integrate_files():
     R.integrate("rk4", 0.03, 3, True, str(d / "ring1000_rk4"))
 
 
+FIXTURES = {"ring1000": ring1000, "ring5000": ring5000, "twowake": twowake, "integrate": integrate_files,
+            "ring1000_ho": ring1000_ho, "twowake_ho": twowake_ho}
+
 if __name__ == "__main__":
-    ring1000()
-    ring5000()
-    twowake()
-    integrate_files()
+    for name in sys.argv[1:] or FIXTURES:
+        FIXTURES[name]()
     for p in sorted(OUT.rglob("*")):
         if p.is_file() and p.suffix != ".py":
             print(p.relative_to(OUT), p.stat().st_size)

@@ -18,6 +18,8 @@ from pawan_b200 import cases, wakeio
 ROOT = Path(__file__).resolve().parents[1]
 GOLD = ROOT / "tests" / "golden"
 DRIVER = ROOT / "tests" / "_build" / "dropin_check"
+# the same driver built against PAWAN compiled with its high-order kernel
+DRIVER_HO = ROOT / "tests" / "_build" / "dropin_check_ho"
 
 
 @pytest.fixture(scope="module")
@@ -128,3 +130,31 @@ def test_dropin_resolve_matches_reference(gpu, driver, resolved_ref, tmp_path, m
     err = np.abs(got - resolved_ref).max() / np.abs(resolved_ref).max()
     print(f"resolve {mode}: max relative strength difference {err:.2e}")
     assert err < tol
+
+
+@pytest.fixture(scope="module")
+def driver_ho():
+    if not DRIVER_HO.exists():
+        pytest.skip("high-order drop-in driver not built (make -C tests/dropin all PAWAN_SRC=<PAWAN tree>)")
+    return DRIVER_HO
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,tol", [("gpu64", 1e-10), ("gpu", 1e-5)])
+def test_dropin_highorder_build_matches_reference(gpu, driver_ho, tmp_path, ref_ho_available, mode, tol):
+    """PAWAN built with highorder.h: __gpu picks the high-order kernel up from
+    the build (pawan_kernel()) and matches __parallel + __rk4 of the same
+    build in PAWAN's own time loop, enstrophy included."""
+    g = np.load(GOLD / "ring1000.npz")
+    w = cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
+    ref, (_, dref) = run(driver_ho, tmp_path, "ref", "rk4", w, 0.01, 3)
+    got, (_, dgot) = run(driver_ho, tmp_path, mode, "rk4", w, 0.01, 3)
+    gold = np.load(GOLD / "ring1000_ho.npz")
+    # the reference run is the high-order one: its first diagnosis record is the fixture's
+    np.testing.assert_allclose(dref[0, 4:], gold["diag"][3:], rtol=1e-10, atol=1e-14)
+    for (t0, a), (t1, b) in zip(got, ref):
+        assert t0 == t1
+        assert O.rel_err(a[0].pos, b[0].pos) < tol
+        assert O.rel_err(a[0].alpha, b[0].alpha) < tol
+    # enstrophy, enstrophyF, KE, KEF
+    np.testing.assert_allclose(dgot[:, 11:15], dref[:, 11:15], rtol=max(tol, 1e-10))

@@ -1,0 +1,297 @@
+"""PAWAN's high-order algebraic kernel (src/interaction/highorder.h).
+
+PAWAN selects its regularisation at compile time (interaction_utils.h:13-20);
+the oracle builds PAWAN's unmodified sources a second time with highorder.h
+(oracle/ref_highorder.h, oracle/_ref/libpawanref_ho.so), and the fixtures
+tests/golden/ring1000_ho.npz and twowake_ho.npz come from that build.  The
+CPU tests pin the FP64 restatement (rs_set_kernel(1)) to those fixtures; the
+GPU tests hold the C ABI with kernel = PGPU_KERNEL_HIGHORDER to the same
+gates as the Gaussian kernel: 1e-10 in FP64 mode, 1e-5 in FP32C mode.
+"""
+import hashlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pawan_b200 import capi, cases
+
+GOLD = Path(__file__).resolve().parent / "golden"
+TOL = {capi.FP64: 1e-10, capi.FP32C: 1e-5}
+PREC = [capi.FP64, capi.FP32C]
+HO = "highorder"
+
+
+def _digest(w):
+    h = hashlib.sha256()
+    for a in (w.pos, w.alpha, w.sigma, w.vol):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def ring1000():
+    g = np.load(GOLD / "ring1000.npz")
+    return cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
+
+
+def two_wakes():
+    g = np.load(GOLD / "twowake.npz")
+    w1 = cases.Wake(g["pos1"], g["alpha1"], g["sigma1"], g["vol1"])
+    w2 = cases.Wake(g["pos2"], g["alpha2"], g["sigma2"], g["vol2"])
+    return w1, w2
+
+
+def ho_gold():
+    return np.load(GOLD / "ring1000_ho.npz")
+
+
+def check_diag(d, vbi, ref, ref_vbi, tol):
+    """Diagnostics against PAWAN's record (interaction.cpp:325-335)."""
+    np.testing.assert_allclose(d[3:9], ref[3:9], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(vbi, ref_vbi, rtol=max(tol, 1e-10), atol=1e-14)
+    # enstrophy, enstrophyF, KE, KEF
+    np.testing.assert_allclose(d[10:14], ref[10:14], rtol=tol)
+    # helicity of a planar ring is a cancelling sum: compare against its scale
+    assert abs(d[9] - ref[9]) < tol * max(abs(ref[9]), 1e-3 * ref[12])
+    assert abs(d[14] - ref[14]) < 1e-9
+
+
+# ---------------------------------------------------------------- oracle (CPU)
+
+def test_fixture_inputs_and_kernel():
+    g = ho_gold()
+    assert str(g["sha256"]) == _digest(cases.ring_stations(stations=40, seed=0))
+    gg = np.load(GOLD / "ring1000.npz")
+    # the fixture is not the Gaussian one: velocities differ at the percent level
+    assert O.rel_err(g["vel"], gg["vel"]) > 1e-3
+    # enstrophy is zero for the Gaussian kernel only
+    assert gg["diag"][10] == 0.0 and g["diag"][10] > 0.0 and g["diag"][11] > 0.0
+
+
+def test_reference_ho_reproduces_golden(ref_ho_available):
+    g = ho_gold()
+    with O.quiet():
+        R = O.RefSystem([ring1000()], float(g["nu"]), kernel=HO)
+        R.solve()
+        v, a = R.rates()
+        d = R.diagnose()
+        R.close()
+    assert O.rel_err(v, g["vel"]) < 1e-14
+    assert O.rel_err(a, g["dalpha"]) < 1e-14
+    np.testing.assert_allclose(d[3:], g["diag"][3:], rtol=1e-12, atol=1e-15)
+
+
+def test_both_pawan_builds_in_one_process(ref_available, ref_ho_available):
+    """The Gaussian and the high-order PAWAN libraries loaded side by side
+    each keep their own kernel."""
+    w = ring1000()
+    with O.quiet():
+        Rg = O.RefSystem([w], 1e-4)
+        Rh = O.RefSystem([w], 1e-4, kernel=HO)
+        Rg.solve()
+        Rh.solve()
+        vg, _ = Rg.rates()
+        vh, _ = Rh.rates()
+        Rg.close()
+        Rh.close()
+    assert O.rel_err(vg, np.load(GOLD / "ring1000.npz")["vel"]) < 1e-14
+    assert O.rel_err(vh, ho_gold()["vel"]) < 1e-14
+
+
+def test_restatement_ho_rates_field_and_diagnostics_vs_golden():
+    g = ho_gold()
+    w = ring1000()
+    v, a = O.restate_rates(w, float(g["nu"]), kernel=HO)
+    assert O.rel_err(v, g["vel"]) < 1e-12
+    assert O.rel_err(a, g["dalpha"]) < 1e-12
+    assert O.rel_err(O.restate_vorticity_field(w, kernel=HO), g["field"]) < 1e-13
+    d, vbi = O.restate_diagnose(w, kernel=HO)
+    ref = g["diag"]
+    assert np.all(np.abs(d[:3] - ref[:3]) < 1e-14)
+    np.testing.assert_allclose(d[3:], ref[3:], rtol=1e-11, atol=1e-15)
+    np.testing.assert_allclose(vbi, g["vbi"], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(O.restate_getvi(w, [0.0, 0.0, 0.0], kernel=HO), g["vbi"], rtol=1e-12, atol=1e-15)
+    # the switch is per call: the Gaussian restatement is unchanged afterwards
+    gg = np.load(GOLD / "ring1000.npz")
+    assert O.rel_err(O.restate_rates(w, float(g["nu"]))[0], gg["vel"]) < 1e-12
+
+
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_restatement_ho_steps_vs_golden(scheme):
+    g = ho_gold()
+    x, al = O.restate_step(ring1000(), float(g["nu"]), scheme, float(g["dt"]), 2, kernel=HO)
+    assert O.rel_err(x, g[f"{scheme}_pos"]) < 1e-13
+    assert O.rel_err(al, g[f"{scheme}_alpha"]) < 1e-12
+
+
+def test_restatement_ho_two_wakes_vs_golden():
+    g = np.load(GOLD / "twowake_ho.npz")
+    w1, w2 = two_wakes()
+    assert str(g["sha256"]) == _digest(w1) + _digest(w2)
+    wc = cases.Wake.concat([w1, w2])
+    v, a = O.restate_rates(wc, float(g["nu"]), kernel=HO)
+    assert O.rel_err(v, np.concatenate([g["vel1"], g["vel2"]])) < 1e-12
+    assert O.rel_err(a, np.concatenate([g["dalpha1"], g["dalpha2"]])) < 1e-12
+    d, _ = O.restate_diagnose(wc, [0, w1.n, wc.n], kernel=HO)
+    np.testing.assert_allclose(d[3:], g["diag"][3:], rtol=1e-11, atol=1e-14)
+
+
+def test_restatement_ho_getvi_vs_reference(ref_ho_available):
+    w = ring1000()
+    pts = np.array([[0.0, 0.8, 0.0], [-0.255, 0.8, 0.02], [1.0, 0.0, 0.1], [2.0, 1.0, -0.5]])
+    with O.quiet():
+        R = O.RefSystem([w], 1e-4, kernel=HO)
+        ref = np.array([R.getvi(p) for p in pts])
+        R.close()
+    got = np.array([O.restate_getvi(w, p, kernel=HO) for p in pts])
+    assert O.rel_err(got, ref) < 1e-13
+
+
+# ---------------------------------------------------------------- GPU
+
+def ctx_with(wakes, precision, nu, systems=None, **kw):
+    c = capi.Context(precision=precision, nu=nu, kernel=capi.HIGHORDER, **kw)
+    ids = [c.add_wake(w.n, systems[i] if systems else 0) for i, w in enumerate(wakes)]
+    for i, w in zip(ids, wakes):
+        c.set_particles(i, w)
+    return c, ids
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", PREC)
+def test_gpu_ho_rates_vs_golden(gpu, prec):
+    g = ho_gold()
+    c, _ = ctx_with([ring1000()], prec, float(g["nu"]))
+    c.solve()
+    v, a = c.rates(0)
+    assert O.rel_err(v, g["vel"]) < TOL[prec]
+    assert O.rel_err(a, g["dalpha"]) < TOL[prec]
+    pairs, full = c.pair_counts()
+    assert pairs == 1000 * 999 and full == pairs  # no far regime for this kernel
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", PREC)
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_gpu_ho_steps_vs_golden(gpu, prec, scheme):
+    g = ho_gold()
+    c, _ = ctx_with([ring1000()], prec, float(g["nu"]))
+    c.step(scheme, float(g["dt"]), 2)
+    c.sync()
+    x, al = c.state(0)
+    assert O.rel_err(x, g[f"{scheme}_pos"]) < TOL[prec]
+    assert O.rel_err(al, g[f"{scheme}_alpha"]) < TOL[prec]
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", PREC)
+def test_gpu_ho_diagnostics_vs_golden(gpu, prec):
+    g = ho_gold()
+    c, _ = ctx_with([ring1000()], prec, float(g["nu"]))
+    d, vbi = c.diagnose(0)
+    check_diag(d, vbi, g["diag"], g["vbi"], TOL[prec])
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", PREC)
+def test_gpu_ho_two_wakes_vs_golden(gpu, prec):
+    g = np.load(GOLD / "twowake_ho.npz")
+    w1, w2 = two_wakes()
+    c, ids = ctx_with([w1, w2], prec, float(g["nu"]))
+    c.solve()
+    v1, a1 = c.rates(ids[0])
+    v2, a2 = c.rates(ids[1])
+    assert O.rel_err(np.concatenate([v1, v2]), np.concatenate([g["vel1"], g["vel2"]])) < TOL[prec]
+    assert O.rel_err(np.concatenate([a1, a2]), np.concatenate([g["dalpha1"], g["dalpha2"]])) < TOL[prec]
+    d, _ = c.diagnose(0)
+    tol = TOL[prec]
+    np.testing.assert_allclose(d[3:9], g["diag"][3:9], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(d[10:14], g["diag"][10:14], rtol=tol)
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", PREC)
+def test_gpu_ho_vorticity_field_and_probe(gpu, prec):
+    """The field and the probe run in FP64 in both modes."""
+    g = ho_gold()
+    w = ring1000()
+    c, _ = ctx_with([w], prec, float(g["nu"]))
+    assert O.rel_err(c.vorticity_field(0), g["field"]) < 1e-12
+    pts = np.array([[0.0, 0.0, 0.0], [0.0, 0.8, 0.0], [-0.255, 0.8, 0.02], [1.0, 0.0, 0.1], [2.0, 1.0, -0.5]])
+    ref = np.array([O.restate_getvi(w, p, kernel=HO) for p in pts])
+    assert O.rel_err(c.probe(pts), ref) < 1e-12
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(128, 1), (128, 2), (256, 1), (256, 2), (64, 2), (128, 4)])
+def test_gpu_ho_every_kernel_shape(gpu, shape):
+    g = ho_gold()
+    for prec in PREC:
+        c, _ = ctx_with([ring1000()], prec, float(g["nu"]), block=shape[0], tpt=shape[1])
+        c.solve()
+        v, a = c.rates(0)
+        assert O.rel_err(v, g["vel"]) < TOL[prec]
+        assert O.rel_err(a, g["dalpha"]) < TOL[prec]
+        c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 31, 257])
+def test_gpu_ho_ragged_sizes(gpu, n):
+    w = cases.ring_stations(stations=40, seed=0).subset(n)
+    vr, ar = O.restate_rates(w, 1e-4, kernel=HO)
+    for prec in PREC:
+        c, _ = ctx_with([w], prec, 1e-4)
+        c.solve()
+        v, a = c.rates(0)
+        if n == 1:
+            assert np.all(v == 0.0) and np.all(a == 0.0)
+        else:
+            assert O.rel_err(v, vr) < TOL[prec]
+            assert O.rel_err(a, ar) < TOL[prec]
+        c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", PREC)
+def test_gpu_ho_large_ring_sampled_vs_restatement(gpu, prec):
+    """200k particles: 512 sampled targets against the FP64 restatement, and
+    the size-independent property that sum_i dalpha_i/dt vanishes: every
+    ordered pair's stretching and diffusion terms are antisymmetric in (t, s)
+    for any radial kernel (interaction_utils.h:492-495, 358-369)."""
+    w = cases.ring_gaussian(stations=1000, per_section=200, seed=1)
+    rows = np.sort(np.random.default_rng(7).choice(w.n, 512, replace=False))
+    vr, ar = O.restate_rates(w, 1e-4, targets=rows, kernel=HO)
+    c, _ = ctx_with([w], prec, 1e-4)
+    c.solve()
+    v, a = c.rates(0)
+    assert O.rel_err(v[rows], vr) < TOL[prec]
+    assert O.rel_err(a[rows], ar) < TOL[prec]
+    tot = np.abs(a.sum(axis=0)).max()
+    scale = np.abs(a).sum(axis=0).max()
+    assert tot <= (1e-12 if prec == capi.FP64 else 1e-6) * scale
+    c.close()
+
+
+@pytest.mark.gpu
+def test_gpu_ho_surrogate_is_refused(gpu):
+    c, _ = ctx_with([cases.ring_stations(stations=40, seed=0)], capi.FP32C, 1e-4)
+    with pytest.raises(capi.PgpuError, match="Gaussian kernel only"):
+        c.surrogate_enable(0)
+    c.close()
+
+
+def test_unknown_kernel_is_rejected():
+    """Host-side checks only: pgpu_create validates the kernel before any
+    CUDA call."""
+    with pytest.raises(KeyError):
+        capi.Context(kernel="lamb-oseen")
+    with pytest.raises(capi.PgpuError) as e:
+        capi.Context(kernel=2)
+    assert e.value.code == capi.PGPU_EINVAL
