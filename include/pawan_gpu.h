@@ -155,6 +155,26 @@ int pgpu_records(pgpu_ctx *ctx, int32_t system, void **P, void **Q);
 int pgpu_influence(pgpu_ctx *ctx);
 int pgpu_get_vorticity_field(pgpu_ctx *ctx, int32_t wake, double *field);
 
+/* Replaces: __wake::merge (wake.cpp:112-159), the O(N^2) half of
+ * __wake::relax (wake.cpp:161-165, called per wake by __interaction::relax,
+ * interaction.cpp:367-371, in the coupled time loop, integration.cpp:87), on
+ * the device state of one wake.  PAWAN's loop visits the particles i whose age
+ * passes `stepnum - _active[i] > 45` up to the first that fails; the caller
+ * passes the length of that prefix as n_elig (it holds the ages).  A particle
+ * j > i within 0.125 (r_i + r_j) of i, with non-zero, non-aligned strength
+ * (1 - cos >= 1e-4), is merged into i: x_i moves to the strength-weighted
+ * mean, alpha_i += alpha_j, alpha_j and vol_j become zero.  The candidate
+ * search runs on the device; the sequential loop, whose every decision
+ * depends on the earlier merges, is replayed on the host over the candidates
+ * in PAWAN's order and arithmetic, and the changed rows are written back.
+ * *nmerged (may be NULL) receives the number of merges.  Wakes of fewer than
+ * 2^31 particles. */
+int pgpu_merge(pgpu_ctx *ctx, int32_t wake, int64_t n_elig, int64_t *nmerged);
+
+/* Replaces: reading __wake::_position, _vorticity, _radius, _volume
+ * (wake.h:49-54) - downloads one wake's particles; any pointer may be NULL. */
+int pgpu_get_particles(pgpu_ctx *ctx, int32_t wake, double *pos, double *alpha, double *sigma, double *vol);
+
 /* Replaces: __interaction::diagnose (interaction.cpp:64-194) for one system.
  * out[15] = total vorticity(3), linear impulse(3), angular impulse(3),
  * helicity, enstrophy, enstrophyF, kinetic energy, kinetic energyF, Zc - the

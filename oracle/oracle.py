@@ -88,6 +88,8 @@ def ref_lib(kernel="gaussian"):
         lib.ref_getvi.argtypes = [C.c_void_p, _dp, _dp]
         lib.ref_influence.argtypes = [C.c_void_p, _dp]
         lib.ref_integrate.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]
+        lib.ref_merge.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int64]
+        lib.ref_get_particles.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
         lib.ref_wtime.restype = C.c_double
         _ref[k] = lib
     return _ref[k]
@@ -157,6 +159,17 @@ class RefSystem:
         self.lib.ref_getvi(self.h, _p(r), _p(out))
         return out
 
+    def merge(self, w: int, active, stepnum: int):
+        """PAWAN's __wake::merge on wake w with birth steps ``active``."""
+        a = _c(active)
+        self.lib.ref_merge(self.h, w, _p(a), int(stepnum))
+
+    def particles(self, w: int = 0):
+        n = self.ns[w]
+        x, a, r, v = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(n)
+        self.lib.ref_get_particles(self.h, w, _p(x), _p(a), _p(r), _p(v))
+        return x, a, r, v
+
     def integrate(self, scheme: str, t: float, n: int, diagnose: bool, path: str):
         self.lib.ref_integrate(self.h, SCHEMES[scheme], float(t), int(n), int(diagnose), str(path).encode())
 
@@ -171,6 +184,8 @@ def restate_lib():
         lib.rs_getvi.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp]
         lib.rs_vorticity_field.argtypes = [C.c_int64, _dp, _dp, _dp, _i64p, C.c_int64, _dp]
         lib.rs_set_kernel.argtypes = [C.c_int]
+        lib.rs_merge.argtypes = [C.c_int64, C.c_int64, _dp, _dp, _dp, _dp]
+        lib.rs_merge.restype = C.c_int64
         lib.rs_threads.restype = C.c_int
         _rs = lib
     return _rs
@@ -242,6 +257,15 @@ def restate_getvi(w, r, kernel="gaussian") -> np.ndarray:
     out = np.zeros(3)
     lib.rs_getvi(w.n, _p(_c(w.pos)), _p(_c(w.alpha)), _p(_c(w.sigma)), _p(_c(r)), _p(out))
     return out
+
+
+def restate_merge(w, n_elig: int):
+    """PAWAN's particle merge over the first n_elig particles of ``w``:
+    returns (pos, alpha, vol, merges), new arrays."""
+    lib = restate_lib()
+    pos, al, vo = _c(w.pos).copy(), _c(w.alpha).copy(), _c(w.vol).copy()
+    m = lib.rs_merge(w.n, int(n_elig), _p(pos), _p(al), _p(_c(w.sigma)), _p(vo))
+    return pos, al, vo, int(m)
 
 
 def restate_threads() -> int:

@@ -215,6 +215,24 @@ void ref_integrate(void *hp, int scheme, double t, int n, int diagnose, const ch
   fflush(NULL);
 }
 
+// PAWAN's own particle merge __wake::merge (wake.cpp:112-159) on wake w, after
+// setting the particles' birth steps (_active) that its age test reads.
+void ref_merge(void *hp, int w, const double *active, int64_t stepnum) {
+  oracle_wake *W = ((handle *)hp)->wakes[w];
+  for (size_t i = 0; i < W->_numParticles; ++i) gsl_vector_set(W->_active, i, active[i]);
+  size_t s = (size_t)stepnum;
+  W->merge(s);
+}
+
+void ref_get_particles(void *hp, int w, double *pos, double *alpha, double *radius, double *volume) {
+  oracle_wake *W = ((handle *)hp)->wakes[w];
+  ref_get_wake(hp, w, pos, alpha);
+  for (size_t i = 0; i < W->_numParticles; ++i) {
+    radius[i] = gsl_vector_get(W->_radius, i);
+    volume[i] = gsl_vector_get(W->_volume, i);
+  }
+}
+
 double ref_wtime(void) { return omp_get_wtime(); }
 
 }  // extern "C"

@@ -303,4 +303,121 @@ void rs_vorticity_field(int64_t n, const double *pos, const double *alpha, const
   }
 }
 
+/* Particle merge, __wake::merge (wake.cpp:112-159), sequential as PAWAN's
+ * loop: for i < n_elig (the age-eligible prefix) and j = i+1 .. n-1 in order,
+ * j merges into i when |x_i - x_j| < 0.125 (r_i + r_j), |a_j| != 0,
+ * |a_i| != 0 (|a_i| taken at the start of i's turn) and
+ * 1 - a_i.a_j / |a_i| / |a_j| >= 1e-4; then
+ * x_i = (x_i |a_i| + x_j |a_j|) (1 / (|a_i| + |a_j|)), a_i += a_j, a_j = 0,
+ * vol_j = 0.  Norms by the scaled sum of squares of gsl_blas_dnrm2.
+ * Instead of PAWAN's O(n^2) j loop, the js are found in a uniform grid of
+ * the positions at entry (cell = 0.25 r_max): only x_i moves during i's turn,
+ * and a j > i has not moved yet.  Each time x_i moves, the js after the last
+ * merged one are gathered again around the new x_i (within
+ * 0.125 (r_i + r_max)) and visited in increasing order, so every merge PAWAN
+ * makes is found in PAWAN's order.  Returns the number of merges; pos, alpha,
+ * vol are updated in place. */
+static double nrm2_3(double a, double b, double c) {
+  const double v[3] = {a, b, c};
+  double scale = 0.0, ssq = 1.0;
+  for (int k = 0; k < 3; ++k) {
+    if (v[k] != 0.0) {
+      const double ax = fabs(v[k]);
+      if (scale < ax) { ssq = 1.0 + ssq * (scale / ax) * (scale / ax); scale = ax; }
+      else ssq += (ax / scale) * (ax / scale);
+    }
+  }
+  return scale * sqrt(ssq);
+}
+
+static int cmp_i64(const void *a, const void *b) {
+  const int64_t x = *(const int64_t *)a, y = *(const int64_t *)b;
+  return x < y ? -1 : x > y;
+}
+
+typedef struct { int64_t key, idx; } cell_ent;
+static int cmp_cell(const void *a, const void *b) {
+  const cell_ent *x = (const cell_ent *)a, *y = (const cell_ent *)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->idx < y->idx ? -1 : x->idx > y->idx;
+}
+
+static int64_t cell_key(int64_t cx, int64_t cy, int64_t cz) {
+  return ((cx & 0x1fffff) << 42) | ((cy & 0x1fffff) << 21) | (cz & 0x1fffff);
+}
+
+int64_t rs_merge(int64_t n, int64_t n_elig, double *pos, double *alpha, const double *sigma, double *vol) {
+  if (n_elig > n) n_elig = n;
+  if (n < 2 || n_elig <= 0) return 0;
+  double rmax = 0.0;
+  for (int64_t i = 0; i < n; ++i) rmax = sigma[i] > rmax ? sigma[i] : rmax;
+  const double h = rmax > 0.0 ? 0.25 * rmax : 1.0;
+  cell_ent *ent = (cell_ent *)malloc(sizeof(cell_ent) * n);
+  for (int64_t i = 0; i < n; ++i) {
+    ent[i].key = cell_key((int64_t)floor(pos[3 * i] / h), (int64_t)floor(pos[3 * i + 1] / h),
+                          (int64_t)floor(pos[3 * i + 2] / h));
+    ent[i].idx = i;
+  }
+  qsort(ent, n, sizeof(cell_ent), cmp_cell);
+  int64_t *js = (int64_t *)malloc(sizeof(int64_t) * n);
+  int64_t merges = 0;
+  for (int64_t i = 0; i < n_elig; ++i) {
+    double *xi = pos + 3 * i, *ai = alpha + 3 * i;
+    const double ivormag = nrm2_3(ai[0], ai[1], ai[2]);
+    if (ivormag == 0.0) continue;
+    const double ri = sigma[i];
+    int64_t after = i;  /* js > after are still to be visited */
+    for (;;) {
+      /* gather the js > after within 0.125 (r_i + r_max) of the current x_i */
+      const double reach = 0.125 * (ri + rmax);
+      const int64_t c0[3] = {(int64_t)floor((xi[0] - reach) / h), (int64_t)floor((xi[1] - reach) / h),
+                             (int64_t)floor((xi[2] - reach) / h)};
+      const int64_t c1[3] = {(int64_t)floor((xi[0] + reach) / h), (int64_t)floor((xi[1] + reach) / h),
+                             (int64_t)floor((xi[2] + reach) / h)};
+      int64_t nj = 0;
+      for (int64_t cx = c0[0]; cx <= c1[0]; ++cx)
+        for (int64_t cy = c0[1]; cy <= c1[1]; ++cy)
+          for (int64_t cz = c0[2]; cz <= c1[2]; ++cz) {
+            const int64_t key = cell_key(cx, cy, cz);
+            int64_t lo = 0, hi = n; /* first entry with this key */
+            while (lo < hi) {
+              const int64_t mid = (lo + hi) / 2;
+              if (ent[mid].key < key) lo = mid + 1; else hi = mid;
+            }
+            for (int64_t e = lo; e < n && ent[e].key == key; ++e)
+              if (ent[e].idx > after) js[nj++] = ent[e].idx;
+          }
+      qsort(js, nj, sizeof(int64_t), cmp_i64);
+      int moved = 0;
+      for (int64_t t = 0; t < nj; ++t) {
+        const int64_t j = js[t];
+        double *xj = pos + 3 * j, *aj = alpha + 3 * j;
+        const double jvormag = nrm2_3(aj[0], aj[1], aj[2]);
+        const double rho = nrm2_3(xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]);
+        if (!(rho < 0.125 * (ri + sigma[j]) && jvormag != 0.0)) continue;
+        const double dot = ai[0] * aj[0] + ai[1] * aj[1] + ai[2] * aj[2];
+        const double alignment = 1 - dot / ivormag / jvormag;
+        if (!(alignment >= 0.0001)) continue;
+        const double s = 1 / (ivormag + jvormag);
+        for (int m = 0; m < 3; ++m) {
+          double p = xi[m] * ivormag;
+          p += xj[m] * jvormag;
+          xi[m] = p * s;
+          ai[m] += aj[m];
+          aj[m] = 0.0;
+        }
+        vol[j] = 0.0;
+        ++merges;
+        after = j;
+        moved = 1;
+        break; /* x_i moved: gather again around it */
+      }
+      if (!moved) break;
+    }
+  }
+  free(js);
+  free(ent);
+  return merges;
+}
+
 int rs_threads(void) { return omp_get_max_threads(); }

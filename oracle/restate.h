@@ -52,6 +52,10 @@ void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *s
  * targets (all if NULL), the target itself included (PAWAN's influence()). */
 void rs_vorticity_field(int64_t n, const double *pos, const double *alpha, const double *sigma,
                         const int64_t *targets, int64_t nt, double *field);
+/* PAWAN's particle merge (__wake::merge, wake.cpp:112-159) over the first
+ * n_elig particles (the age-eligible prefix of PAWAN's loop); pos, alpha and
+ * vol are updated in place.  Returns the number of merges. */
+int64_t rs_merge(int64_t n, int64_t n_elig, double *pos, double *alpha, const double *sigma, double *vol);
 int rs_threads(void);
 
 #ifdef __cplusplus

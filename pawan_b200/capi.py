@@ -42,7 +42,8 @@ EXPORTS = [
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
     "pgpu_rates_noalloc", "pgpu_noalloc_last_error", "pgpu_set_target_range", "pgpu_stage", "pgpu_records",
-    "pgpu_sync_timeout", "pgpu_set_timing", "pgpu_influence", "pgpu_get_vorticity_field",
+    "pgpu_sync_timeout", "pgpu_set_timing", "pgpu_influence", "pgpu_get_vorticity_field", "pgpu_merge",
+    "pgpu_get_particles",
 ]
 
 
@@ -155,6 +156,8 @@ def load(build_if_missing: bool = False):
         "pgpu_set_timing": (C.c_int, [vp, C.c_int]),
         "pgpu_influence": (C.c_int, [vp]),
         "pgpu_get_vorticity_field": (C.c_int, [vp, C.c_int32, _dp]),
+        "pgpu_merge": (C.c_int, [vp, C.c_int32, C.c_int64, _i64p]),
+        "pgpu_get_particles": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -314,6 +317,21 @@ class Context:
             self._ck(self.lib.pgpu_sync(self.h))
         else:
             self._ck(self.lib.pgpu_sync_timeout(self.h, float(timeout)))
+
+    def merge(self, wake: int, n_elig: int) -> int:
+        """PAWAN's particle merge (__wake::merge) over the wake's first n_elig
+        particles (those old enough to merge); returns the number of merges."""
+        m = C.c_int64(0)
+        self._ck(self.lib.pgpu_merge(self.h, wake, int(n_elig), C.byref(m)))
+        return int(m.value)
+
+    def particles(self, wake: int = 0):
+        """(pos, alpha, sigma, vol) of a wake."""
+        n = self.num_particles(wake)
+        pos, alpha = np.zeros((n, 3)), np.zeros((n, 3))
+        sigma, vol = np.zeros(n), np.zeros(n)
+        self._ck(self.lib.pgpu_get_particles(self.h, wake, _p(pos), _p(alpha), _p(sigma), _p(vol)))
+        return pos, alpha, sigma, vol
 
     def vorticity_field(self, wake: int = 0) -> np.ndarray:
         """PAWAN's influence(): the vorticity field (n x 3) at the wake's particles

@@ -198,3 +198,77 @@ class RotorShedder:
         seglen = np.linalg.norm(alpha, axis=1) / self.gamma
         self.step_index += 1
         return Wake(pos, alpha, np.full(pos.shape[0], self.sigma), seglen * math.pi * self.core ** 2)
+
+
+def _rotate(v: np.ndarray, axis: np.ndarray, theta: float) -> np.ndarray:
+    axis = axis / np.linalg.norm(axis)
+    return v * math.cos(theta) + np.cross(axis, v) * math.sin(theta) + axis * np.dot(axis, v) * (1 - math.cos(theta))
+
+
+def merge_clusters(stations: int = 40, clusters: int = 150, chains: int = 10, seed: int = 0,
+                   young: float = 0.2) -> tuple[Wake, int, np.ndarray]:
+    """A wake for PAWAN's particle merge (``__wake::merge``, wake.cpp:112-159).
+
+    A ``ring_stations`` ring with, around random ring particles, 1-3 extra
+    particles each at 0.2-1.4 times the merge reach 0.125 (r_i + r_j), with
+    strengths rotated by 0, 0.005, 0.02, 0.3, 1.5 or 3 rad (PAWAN merges when
+    1 - cos >= 1e-4) and scaled by 0.3-4; 20 zero-strength particles; all of
+    it shuffled.  In front of it, ``chains`` lines of 6 particles 0.2 r apart
+    whose strengths are each perpendicular to the sum of the ones before: the
+    head absorbs them one by one and ends up more than twice the merge reach
+    from where it started.  Returns (wake, n_elig, active): PAWAN's loop visits
+    particles while ``stepnum - active > 45``; with stepnum 100 the first
+    n_elig = (1 - young) n particles qualify, the next one does not.
+    """
+    rng = np.random.default_rng(seed)
+    b = ring_stations(stations=stations, seed=seed)
+    r = float(b.sigma[0])
+    reach = 0.25 * r
+    P, A, S, V = [b.pos], [b.alpha], [b.sigma], [b.vol]
+    for _ in range(clusters):
+        i = rng.integers(b.n)
+        for _ in range(rng.integers(1, 4)):
+            off = rng.normal(size=3)
+            off *= rng.uniform(0.2, 1.4) * reach / np.linalg.norm(off)
+            th = float(rng.choice([0.0, 0.005, 0.02, 0.3, 1.5, 3.0]))
+            a = _rotate(b.alpha[i], rng.normal(size=3), th) * rng.uniform(0.3, 4.0)
+            P.append((b.pos[i] + off)[None]); A.append(a[None]); S.append([r]); V.append([b.vol[i]])
+    for _ in range(20):
+        i = rng.integers(b.n)
+        P.append((b.pos[i] + 0.01 * r)[None]); A.append(np.zeros((1, 3))); S.append([r]); V.append([1e-4])
+    pos, alpha = np.concatenate(P), np.concatenate(A)
+    sig, vol = np.concatenate(S).astype(float), np.concatenate(V).astype(float)
+    perm = rng.permutation(pos.shape[0])
+    pos, alpha, sig, vol = pos[perm], alpha[perm], sig[perm], vol[perm]
+    cp, ca = [], []
+    for _ in range(chains):
+        x0 = rng.uniform(-1.5, 1.5, 3) + np.array([0.0, 0.0, 2.0])
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        tot = rng.normal(size=3) * 1e-3
+        cp.append(x0); ca.append(tot.copy())
+        for k in range(1, 6):
+            u = np.cross(tot, rng.normal(size=3))
+            u *= 1e-2 / np.linalg.norm(u)
+            cp.append(x0 + k * 0.2 * r * d); ca.append(u)
+            tot = tot + u
+    nc = len(cp)
+    w = Wake(np.concatenate([np.array(cp).reshape(-1, 3), pos]), np.concatenate([np.array(ca).reshape(-1, 3), alpha]),
+             np.concatenate([np.full(nc, r), sig]), np.concatenate([np.full(nc, 1e-4), vol]))
+    n_elig = int((1.0 - young) * w.n)
+    active = np.zeros(w.n)
+    if n_elig < w.n:
+        active[n_elig] = 90.0
+        active[n_elig + 1:] = rng.choice([0.0, 90.0], w.n - n_elig - 1)
+    return w, n_elig, active
+
+
+def jittered(w: Wake, theta: float, seed: int = 0) -> Wake:
+    """``w`` with every strength rotated by ``theta`` about a random axis."""
+    rng = np.random.default_rng(seed)
+    ax = rng.normal(size=w.alpha.shape)
+    ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+    a = w.alpha
+    c, s = math.cos(theta), math.sin(theta)
+    rot = a * c + np.cross(ax, a) * s + ax * (ax * a).sum(1, keepdims=True) * (1 - c)
+    return Wake(w.pos.copy(), np.ascontiguousarray(rot), w.sigma.copy(), w.vol.copy())

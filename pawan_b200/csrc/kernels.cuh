@@ -23,6 +23,7 @@
 // bit-reproducible run to run.
 #pragma once
 #include <cuda_runtime.h>
+#include <math_constants.h>
 #include <stdint.h>
 
 #include "pair_math.cuh"
@@ -901,6 +902,78 @@ static __global__ void diag_wake_kernel(const double *x0, const double *sig, con
   for (int m = 0; m < kDiagFields; ++m) {
     const double r = block_sum(f[m], red);
     if (threadIdx.x == 0) out[(int64_t)blockIdx.x * kDiagFields + m] = r;
+  }
+}
+
+// Candidate pairs of PAWAN's particle merge (__wake::merge, wake.cpp:112-159).
+// PAWAN merges j into i (i < j) when |x_i - x_j| < 0.125 (r_i + r_j), both
+// strengths are non-zero and the strengths are not aligned; its loop is
+// sequential (a merge moves x_i and zeroes alpha_j), so the host replays it
+// (pgpu_merge).  This kernel does the O(N^2) part: every pair of one wake with
+// i < n_elig, i < j < n, non-zero strengths at entry and
+// |x_i - x_j| < reach (r_i + r_j) at entry, reach = 0.25, twice PAWAN's, so
+// the host can keep using the list while a merged x_i stays within
+// 0.125 (r_i + r_min) of where it started.  A zero strength is staged as a NaN
+// radius, which fails the distance test.  Pairs are packed
+// (i << 32 | j << 1 | out), wake indices, so that sorting the keys orders them
+// by i, then j; out = 1 marks a pair surely outside PAWAN's reach at entry
+// (|x_i - x_j|^2 >= (0.125 (r_i + r_j))^2 (1 + 1e-12), a margin far above the
+// rounding of either side's distance), which cannot merge before x_i has
+// moved.  count may exceed max_pairs, and then only the first max_pairs are
+// stored (the host retries with room for all of them).
+struct MergeArgs {
+  const double *x0;  // [6][cap] state
+  const double *sig;
+  int64_t cap, off, n, n_elig;
+  double reach;
+  unsigned long long *pairs;
+  unsigned long long *count;
+  int64_t max_pairs;
+};
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) merge_candidates_kernel(MergeArgs a) {
+  __shared__ double4 sP[BLOCK];
+  const int64_t cap = a.cap;
+  const int64_t i = blockIdx.x * (int64_t)BLOCK + threadIdx.x;
+  const bool vi = i < a.n_elig;
+  double xi = 0, yi = 0, zi = 0, ri = CUDART_NAN;
+  if (vi) {
+    const int64_t g = a.off + i;
+    xi = a.x0[g]; yi = a.x0[cap + g]; zi = a.x0[2 * cap + g];
+    const bool nz = a.x0[3 * cap + g] != 0.0 || a.x0[4 * cap + g] != 0.0 || a.x0[5 * cap + g] != 0.0;
+    ri = nz ? a.sig[g] : CUDART_NAN;
+  }
+  // sources: tiles from this CTA's first target on, split over gridDim.y
+  const int64_t first = blockIdx.x * (int64_t)BLOCK;
+  const int64_t tiles = (a.n - first + BLOCK - 1) / BLOCK;
+  for (int64_t t = blockIdx.y; t < tiles; t += gridDim.y) {
+    const int64_t jb = first + t * BLOCK;
+    __syncthreads();
+    const int64_t j = jb + threadIdx.x;
+    if (j < a.n) {
+      const int64_t g = a.off + j;
+      const bool nz = a.x0[3 * cap + g] != 0.0 || a.x0[4 * cap + g] != 0.0 || a.x0[5 * cap + g] != 0.0;
+      sP[threadIdx.x] = make_double4(a.x0[g], a.x0[cap + g], a.x0[2 * cap + g], nz ? a.sig[g] : CUDART_NAN);
+    } else {
+      sP[threadIdx.x] = make_double4(0.0, 0.0, 0.0, CUDART_NAN);
+    }
+    __syncthreads();
+    if (!vi) continue;
+    const int cnt = (int)min((int64_t)BLOCK, a.n - jb);
+    for (int jj = 0; jj < cnt; ++jj) {
+      const double4 p = sP[jj];
+      const double dx = xi - p.x, dy = yi - p.y, dz = zi - p.z;
+      const double lim = a.reach * (ri + p.w);
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (jb + jj > i && d2 < lim * lim) {
+        const double pawan = 0.125 * (ri + p.w);
+        const unsigned long long out = d2 >= pawan * pawan * (1.0 + 1e-12) ? 1ull : 0ull;
+        const unsigned long long k = atomicAdd(a.count, 1ull);
+        if ((int64_t)k < a.max_pairs)
+          a.pairs[k] = ((unsigned long long)i << 32) | ((unsigned long long)(jb + jj) << 1) | out;
+      }
+    }
   }
 }
 

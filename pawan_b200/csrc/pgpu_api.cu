@@ -89,6 +89,10 @@ struct pgpu_ctx {
   int64_t *d_sysoff = nullptr, *d_sysn = nullptr, *d_syst = nullptr;
   PlanEntry *d_plan = nullptr, *d_plan_diag = nullptr, *d_plan_field = nullptr;
   double *d_field = nullptr;  // [6][cap] vorticity field (components 0..2), allocated by pgpu_influence
+  unsigned long long *d_merge = nullptr;  // merge candidate keys (pgpu_merge): d_merge_cap, a counter, d_merge_cap sorted
+  int64_t d_merge_cap = 0;
+  void *d_merge_tmp = nullptr;  // radix-sort space of the candidate keys
+  size_t d_merge_tmp_bytes = 0;
   unsigned int *d_counters = nullptr;
   unsigned long long *d_nfull = nullptr;
   int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
@@ -505,7 +509,7 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
                   c->d_sysoff, c->d_sysn, c->d_syst, c->d_plan, c->d_plan_diag, c->d_plan_field, c->d_field,
-                  c->d_counters, c->d_nfull, c->d_flag};
+                  c->d_counters, c->d_nfull, c->d_flag, c->d_merge, c->d_merge_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
@@ -1044,3 +1048,4 @@ const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err.c_str() : "null con
 
 #include "mlp_host.inc"
 #include "surrogate_host.inc"
+#include "merge_host.inc"

@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
     const int t = min(t0, tc.end - 1);
     const float4 pt = a.Ps[t], qt = a.Qs[t];
     const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
-    const float hst = pt.w, h50 = kFarU * pt.w, vt = qt.w;
+    const float hst = pt.w, vt = qt.w;
     float vh[3] = {0, 0, 0}, vl[3] = {0, 0, 0}, dh[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
     const int fo = a.far_off[li], fn = a.far_cnt[li];
     for (int c0 = 0; c0 < fn; c0 += kWarpCells) {

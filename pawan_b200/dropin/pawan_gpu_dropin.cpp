@@ -102,6 +102,21 @@ void __gpu::diagnose() {
   _Zc = out[14];
 }
 
+void __gpu::relax(size_t &stepnum) {
+  for (__wake *W : _wakes) W->split(stepnum);
+  upload();  // split may have appended particles
+  for (size_t k = 0; k < _wakes.size(); ++k) {
+    __wake *W = _wakes[k];
+    // PAWAN's merge loop visits particles while they pass its age test (wake.cpp:115)
+    int64_t n_elig = 0;
+    while ((size_t)n_elig < W->_numParticles && stepnum - gsl_vector_get(W->_active, n_elig) > 45) ++n_elig;
+    int64_t merged = 0;
+    check(pgpu_merge(_ctx, _ids[k], n_elig, &merged));
+    if (merged)
+      check(pgpu_get_particles(_ctx, _ids[k], W->_position->data, W->_vorticity->data, nullptr, W->_volume->data));
+  }
+}
+
 // __interaction::influence (interaction.cpp:212-260): zeroes every wake's
 // _vorticityfield and fills it with the field from all wakes (the particle
 // itself included, as SELFINFLUENCE adds it).

@@ -61,6 +61,11 @@ class __gpu : public __interaction {
   void addWake(__wake *W) override;
   void solve() override;
   void diagnose() override;
+  // __interaction::relax (interaction.cpp:367-371), each wake's split then
+  // merge (wake.cpp:161-165): PAWAN's own O(N) split on the host wake, then
+  // the O(N^2) merge through pgpu_merge (candidates on the device, PAWAN's
+  // sequential loop replayed on the host), written back to the host wake.
+  void relax(size_t &stepnum) override;
 
   // Advances the wakes `nsteps` steps on the device (scheme PGPU_RK3 / PGPU_RK4
   // / PGPU_EULER) starting from the host wakes, then writes the new state back

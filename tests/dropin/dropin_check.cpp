@@ -15,6 +15,18 @@
 // to <out-prefix>.strengths:
 //
 //   dropin_check resolve ref|gpu|gpu64 <nLayers> <nAzi> <sigma> <out-prefix>
+//
+// A third mode runs PAWAN's relaxation __interaction::relax(stepnum)
+// (interaction.cpp:367-371: each wake's split, then merge, wake.cpp:61-165)
+// once, with either backend, on particles read from a file:
+//
+//   dropin_check relax ref|gpu|gpu64 <particles.bin> <ages.bin> <stepnum> <out-prefix>
+//
+// ages.bin: int64 n, then n birth steps (_active) and n birth strengths.  The
+// wake is laid out as in the coupled run (__wake::initialise_memory,
+// wake.cpp:27-44: MAXNUMPARTICLES rows, _npidx = n) so split can append.
+// Output <out-prefix>.relax: int64 n, then n*3 positions, n*3 strengths,
+// n radii, n volumes, n birth strengths, n birth steps (FP64).
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -44,6 +56,29 @@ struct file_wake : public pawan::__wake {
       gsl_vector_set(_radius, i, d[6 * n + i]);
       gsl_vector_set(_volume, i, d[7 * n + i]);
     }
+  }
+};
+
+// A wake with PAWAN's coupled-run layout (capacity MAXNUMPARTICLES) holding n particles.
+struct coupled_wake : public pawan::__wake {
+  coupled_wake(const std::vector<double> &d, const std::vector<double> &ages, int64_t n) : pawan::__wake() {
+    gsl_matrix_free(_position); gsl_matrix_free(_velocity); gsl_matrix_free(_vorticity);
+    gsl_matrix_free(_retvorcity); gsl_vector_free(_radius); gsl_vector_free(_volume);
+    gsl_vector_free(_birthstrength); gsl_matrix_free(_vorticityfield); gsl_vector_free(_active);
+    initialise_memory();
+    for (int64_t i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) {
+        gsl_matrix_set(_position, i, k, d[3 * i + k]);
+        gsl_matrix_set(_vorticity, i, k, d[3 * n + 3 * i + k]);
+      }
+      gsl_vector_set(_radius, i, d[6 * n + i]);
+      gsl_vector_set(_volume, i, d[7 * n + i]);
+      gsl_vector_set(_active, i, ages[i]);
+      gsl_vector_set(_birthstrength, i, ages[n + i]);
+    }
+    _npidx = (size_t)n;
+    _numParticles = (size_t)n;
+    _size = 2 * _numParticles * 3;
   }
 };
 
@@ -92,8 +127,61 @@ int run_resolve(int argc, char **argv) {
   return 0;
 }
 
+static bool read_doubles(const char *path, int64_t per, std::vector<double> &d, int64_t &n) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return false;
+  bool ok = fread(&n, sizeof(n), 1, f) == 1 && n >= 0;
+  if (ok) {
+    d.resize((size_t)(per * n));
+    ok = fread(d.data(), sizeof(double), d.size(), f) == d.size();
+  }
+  fclose(f);
+  return ok;
+}
+
+int run_relax(int argc, char **argv) {
+  if (argc < 7) {
+    fprintf(stderr, "usage: %s relax ref|gpu|gpu64 particles.bin ages.bin stepnum out\n", argv[0]);
+    return 2;
+  }
+  const std::string backend = argv[2];
+  std::vector<double> d, ages;
+  int64_t n = 0, na = 0;
+  if (!read_doubles(argv[3], 8, d, n) || !read_doubles(argv[4], 2, ages, na) || na != n) return 3;
+  coupled_wake W(d, ages, n);
+  pawan::__interaction *S = nullptr;
+  if (backend == "ref") {
+    S = new ref_parallel(&W, 1e-4);
+  } else {
+    pgpu_config cfg;
+    pgpu_config_default(&cfg);
+    cfg.nu = 1e-4;
+    cfg.precision = backend == "gpu64" ? PGPU_FP64 : PGPU_FP32C;
+    S = new pawan::__gpu(&W, cfg);
+  }
+  size_t stepnum = (size_t)atoll(argv[5]);
+  S->relax(stepnum);
+  FILE *f = fopen((std::string(argv[6]) + ".relax").c_str(), "wb");
+  if (!f) return 3;
+  const int64_t m = (int64_t)W._numParticles;
+  fwrite(&m, sizeof(m), 1, f);
+  for (int64_t i = 0; i < m; ++i)
+    for (int k = 0; k < 3; ++k) { double v = gsl_matrix_get(W._position, i, k); fwrite(&v, sizeof(v), 1, f); }
+  for (int64_t i = 0; i < m; ++i)
+    for (int k = 0; k < 3; ++k) { double v = gsl_matrix_get(W._vorticity, i, k); fwrite(&v, sizeof(v), 1, f); }
+  for (int64_t i = 0; i < m; ++i) { double v = gsl_vector_get(W._radius, i); fwrite(&v, sizeof(v), 1, f); }
+  for (int64_t i = 0; i < m; ++i) { double v = gsl_vector_get(W._volume, i); fwrite(&v, sizeof(v), 1, f); }
+  for (int64_t i = 0; i < m; ++i) { double v = gsl_vector_get(W._birthstrength, i); fwrite(&v, sizeof(v), 1, f); }
+  for (int64_t i = 0; i < m; ++i) { double v = gsl_vector_get(W._active, i); fwrite(&v, sizeof(v), 1, f); }
+  fclose(f);
+  fflush(NULL);
+  delete S;
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc > 1 && std::string(argv[1]) == "resolve") return run_resolve(argc, argv);
+  if (argc > 1 && std::string(argv[1]) == "relax") return run_relax(argc, argv);
   if (argc < 7) {
     fprintf(stderr, "usage: %s ref|gpu|gpu64 rk4|rk3 particles.bin dt nsteps out [nu]\n", argv[0]);
     return 2;

@@ -158,3 +158,36 @@ def test_dropin_highorder_build_matches_reference(gpu, driver_ho, tmp_path, ref_
         assert O.rel_err(a[0].alpha, b[0].alpha) < tol
     # enstrophy, enstrophyF, KE, KEF
     np.testing.assert_allclose(dgot[:, 11:15], dref[:, 11:15], rtol=max(tol, 1e-10))
+
+
+def _relax(driver, tmp_path, backend, w, ages, birth, stepnum):
+    pb, ab = tmp_path / "particles.bin", tmp_path / "ages.bin"
+    wakeio.write_particles_bin(pb, w)
+    with open(ab, "wb") as f:
+        np.array([w.n], dtype=np.int64).tofile(f)
+        np.concatenate([ages, birth]).astype(np.float64).tofile(f)
+    out = tmp_path / f"relax_{backend}"
+    r = subprocess.run([str(driver), "relax", backend, str(pb), str(ab), str(stepnum), str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    raw = np.fromfile(str(out) + ".relax")
+    n = int(raw[:1].view(np.int64)[0])
+    v = raw[1:]
+    return n, v
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["gpu64", "gpu"])
+def test_dropin_relax_matches_reference(gpu, driver, tmp_path, ref_available, mode):
+    """PAWAN's relaxation __interaction::relax (split, then merge) through
+    __gpu (split on the host wake, merge through pgpu_merge) against
+    __parallel's, on a coupled-run wake layout: every array equal to the bit."""
+    w, n_elig, active = cases.merge_clusters(seed=2)
+    # a fifth of the eligible particles have grown to 2.5x their birth strength and split
+    rng = np.random.default_rng(8)
+    mag = np.linalg.norm(w.alpha, axis=1)
+    birth = np.where(rng.random(w.n) < 0.2, mag / 2.5, mag)
+    n_ref, ref = _relax(driver, tmp_path, "ref", w, active, birth, 100)
+    n_got, got = _relax(driver, tmp_path, mode, w, active, birth, 100)
+    assert n_got == n_ref > w.n  # split appended particles
+    np.testing.assert_array_equal(got, ref)
