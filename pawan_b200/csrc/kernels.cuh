@@ -623,8 +623,8 @@ template <typename T> struct DiagArgs {
 // unordered pairs.  In FP32 the Gaussian helicity's q takes the far limit
 // 1/rho^3 for u >= 50 (as in the rate kernel) and the mid/series terms only
 // when some lane of the warp needs them.
-template <typename T, int BLOCK, int KER = kGaussian>
-__global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
+template <typename T, int BLOCK, int KER>
+__device__ __forceinline__ void diag_body_generic(const DiagArgs<T> &a) {
   __shared__ __align__(16) v4_t<T> sP[BLOCK];
   __shared__ __align__(16) v4_t<T> sQ[BLOCK];
   __shared__ int s_item;
@@ -723,6 +723,19 @@ __global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
       }
     }
   }
+}
+
+}  // namespace pgpu
+
+#include "diag_f32.cuh"
+
+namespace pgpu {
+
+// The FP32 Gaussian diagnostics take the packed body of diag_f32.cuh.
+template <typename T, int BLOCK, int KER = kGaussian>
+__global__ void __launch_bounds__(BLOCK) diag_pair_kernel(DiagArgs<T> a) {
+  if constexpr (sizeof(T) == 4 && KER == kGaussian) diag_body_f32<BLOCK>(a);
+  else diag_body_generic<T, BLOCK, KER>(a);
 }
 
 // Vorticity field at every particle, PAWAN's influence() (interaction.cpp:
