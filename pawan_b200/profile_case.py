@@ -3,6 +3,8 @@
     python -m pawan_b200.profile_case [--stations 200] [--solves 3] [--fp64] [--steps 1] [--block 256 --tpt 2]
     python -m pawan_b200.profile_case --surrogate 200000 [--solves 2]
     python -m pawan_b200.profile_case --mlp-train 20
+    python -m pawan_b200.profile_case --kernel highorder [--stations 200]
+    python -m pawan_b200.profile_case --merge [--stations 200]
 
 Builds the Gaussian-core vortex ring of the 1M-particle benchmark with
 ``stations`` x 1000 particles (200 -> N = 200,000), runs ``solves`` rate
@@ -30,7 +32,13 @@ def main() -> None:
                     help="instead: octree far field (order 2) on two coaxial rings of this many particles")
     ap.add_argument("--mlp-train", type=int, default=0,
                     help="instead: this many training steps of the far-field network (batch 65536)")
+    ap.add_argument("--kernel", choices=sorted(capi.KERNELS), default="gaussian", help="regularisation kernel")
+    ap.add_argument("--merge", action="store_true",
+                    help="instead: one particle merge (pgpu_merge) of the ring with strengths turned 0.02 rad")
     a = ap.parse_args()
+    if a.merge:
+        merge_case(a.stations)
+        return
     if a.surrogate:
         surrogate_case(a.surrogate, a.solves)
         return
@@ -38,7 +46,8 @@ def main() -> None:
         mlp_case(a.mlp_train)
         return
     w = cases.ring_gaussian(stations=a.stations, per_section=1000, sigma=a.sigma, seed=1)
-    c = capi.Context(precision=capi.FP64 if a.fp64 else capi.FP32C, nu=1e-4, block=a.block, tpt=a.tpt)
+    c = capi.Context(precision=capi.FP64 if a.fp64 else capi.FP32C, nu=1e-4, block=a.block, tpt=a.tpt,
+                     kernel=a.kernel)
     k = c.add_wake(w.n)
     c.set_particles(k, w)
     for _ in range(a.solves):
@@ -56,6 +65,19 @@ def main() -> None:
     t = time.perf_counter()
     d, vbi = c.diagnose(0)
     print(f"diagnose {1e3 * (time.perf_counter() - t):.1f} ms; diagnostics", d.tolist(), "vbi", vbi.tolist())
+    c.close()
+
+
+def merge_case(stations: int) -> None:
+    import time
+    w = cases.jittered(cases.ring_gaussian(stations=stations, per_section=1000, seed=1), 0.02, seed=1)
+    c = capi.Context(precision=capi.FP32C, nu=1e-4)
+    k = c.add_wake(w.n)
+    c.set_particles(k, w)
+    c.sync()
+    t = time.perf_counter()
+    m = c.merge(k, w.n)
+    print(f"N {w.n} merge: {m} merges in {1e3 * (time.perf_counter() - t):.1f} ms")
     c.close()
 
 
