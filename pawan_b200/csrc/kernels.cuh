@@ -806,10 +806,10 @@ __global__ void __launch_bounds__(BLOCK) field_kernel(FieldArgs a) {
         const double s2 = hst + p.w;
         double z = 0.0;
         if constexpr (KER == kHighOrder) {
-          const double is = 1.0 / sqrt(s2);
-          const double iw = 1.0 / sqrt(r2 / s2 + 1.0);
-          const double iw2 = iw * iw;
-          z = (HighOrder::kZeta * kInv4Pi) * (is * is * is) * (iw2 * iw2 * iw2 * iw);
+          // 1.875 / (pi sigma^3 (rho^2/sigma^2 + 1)^3.5) = 1.875 / pi sigma^4 (rho^2 + sigma^2)^-3.5
+          const double iR = 1.0 / sqrt(r2 + s2);
+          const double iR2 = iR * iR;
+          z = (HighOrder::kZeta * kInv4Pi) * (s2 * s2) * (iR2 * iR2 * iR2 * iR);
         } else {
           const bool live = r2 < 1500.0 * s2;
           if (__any_sync(0xffffffffu, live)) z = kInv2Pi15 / (s2 * sqrt(s2)) * exp(-0.5 * r2 / s2);
@@ -922,72 +922,115 @@ static __global__ void diag_wake_kernel(const double *x0, const double *sig, con
 // PAWAN merges j into i (i < j) when |x_i - x_j| < 0.125 (r_i + r_j), both
 // strengths are non-zero and the strengths are not aligned; its loop is
 // sequential (a merge moves x_i and zeroes alpha_j), so the host replays it
-// (pgpu_merge).  This kernel does the O(N^2) part: every pair of one wake with
-// i < n_elig, i < j < n, non-zero strengths at entry and
-// |x_i - x_j| < reach (r_i + r_j) at entry, reach = 0.25, twice PAWAN's, so
-// the host can keep using the list while a merged x_i stays within
-// 0.125 (r_i + r_min) of where it started.  A zero strength is staged as a NaN
-// radius, which fails the distance test.  Pairs are packed
-// (i << 32 | j << 1 | out), wake indices, so that sorting the keys orders them
-// by i, then j; out = 1 marks a pair surely outside PAWAN's reach at entry
-// (|x_i - x_j|^2 >= (0.125 (r_i + r_j))^2 (1 + 1e-12), a margin far above the
-// rounding of either side's distance), which cannot merge before x_i has
-// moved.  count may exceed max_pairs, and then only the first max_pairs are
-// stored (the host retries with room for all of them).
+// (pgpu_merge).  These kernels find, from the state at entry, every pair with
+// i < n_elig, i < j < n, non-zero strengths and
+// |x_i - x_j| < reach (r_i + r_j), reach = 0.25, twice PAWAN's, so the host can
+// keep using the list while a merged x_i stays within 0.125 (r_i + r_min) of
+// where it started.
+//
+// Search: a uniform grid of cell size h = 2 reach r_max.  merge_keys_kernel
+// gives every particle with a non-zero strength its cell key (zero strengths
+// get a key above every cell's, so no search finds them); the keys are sorted
+// with their indices and merge_gather_kernel copies (x, y, z, r) into key
+// order.  merge_grid_kernel then scans, for each i, the cells covering
+// [x_i - reach (r_i + r_max), x_i + reach (r_i + r_max)] in every axis (at
+// most 3 per axis; floor(x / h) is monotonic in x, so no pair within reach is
+// missed at a cell boundary), finding each cell's run of sorted keys by
+// binary search.  Cell coordinates are wrapped to 21 bits per axis in the key;
+// far cells that share a key only add pairs the distance test rejects.
+//
+// Pairs are packed (i << 32 | j << 1 | out), wake indices, so that sorting the
+// keys orders them by i, then j; out = 1 marks a pair surely outside PAWAN's
+// reach at entry (|x_i - x_j|^2 >= (0.125 (r_i + r_j))^2 (1 + 1e-12), a
+// margin far above the rounding of either side's distance), which cannot
+// merge before x_i has moved.  count may exceed max_pairs, and then only the
+// first max_pairs are stored (the host retries with room for all of them).
+constexpr unsigned long long kMergeNoCell = ~0ull;
+
+__device__ __forceinline__ int64_t merge_cell(double x, double h) {
+  return (int64_t)fmin(fmax(floor(x / h), -4.0e18), 4.0e18);
+}
+__device__ __forceinline__ unsigned long long merge_cell_key(int64_t cx, int64_t cy, int64_t cz) {
+  const unsigned long long m = (1ull << 21) - 1;
+  return (((unsigned long long)cx & m) << 42) | (((unsigned long long)cy & m) << 21) | ((unsigned long long)cz & m);
+}
+__device__ __forceinline__ bool merge_nonzero(const double *x0, int64_t cap, int64_t g) {
+  return x0[3 * cap + g] != 0.0 || x0[4 * cap + g] != 0.0 || x0[5 * cap + g] != 0.0;
+}
+
+static __global__ void merge_keys_kernel(const double *x0, int64_t cap, int64_t off, int64_t n, double h,
+                                         unsigned long long *keys, int *idx) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = off + j;
+    keys[j] = merge_nonzero(x0, cap, g)
+                  ? merge_cell_key(merge_cell(x0[g], h), merge_cell(x0[cap + g], h), merge_cell(x0[2 * cap + g], h))
+                  : kMergeNoCell;
+    idx[j] = (int)j;
+  }
+}
+
+// (x, y, z, r) of the particles in sorted key order.
+static __global__ void merge_gather_kernel(const double *x0, const double *sig, int64_t cap, int64_t off, int64_t n,
+                                           const int *idx, double4 *rec) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = off + idx[e];
+    rec[e] = make_double4(x0[g], x0[cap + g], x0[2 * cap + g], sig[g]);
+  }
+}
+
 struct MergeArgs {
   const double *x0;  // [6][cap] state
   const double *sig;
   int64_t cap, off, n, n_elig;
-  double reach;
+  double reach, h, rmax;
+  const unsigned long long *keys;  // sorted cell keys
+  const int *idx;                  // particle of each sorted key
+  const double4 *rec;              // (x, y, z, r) in sorted key order
   unsigned long long *pairs;
   unsigned long long *count;
   int64_t max_pairs;
 };
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) merge_candidates_kernel(MergeArgs a) {
-  __shared__ double4 sP[BLOCK];
-  const int64_t cap = a.cap;
-  const int64_t i = blockIdx.x * (int64_t)BLOCK + threadIdx.x;
-  const bool vi = i < a.n_elig;
-  double xi = 0, yi = 0, zi = 0, ri = CUDART_NAN;
-  if (vi) {
-    const int64_t g = a.off + i;
-    xi = a.x0[g]; yi = a.x0[cap + g]; zi = a.x0[2 * cap + g];
-    const bool nz = a.x0[3 * cap + g] != 0.0 || a.x0[4 * cap + g] != 0.0 || a.x0[5 * cap + g] != 0.0;
-    ri = nz ? a.sig[g] : CUDART_NAN;
+static __global__ void merge_grid_kernel(MergeArgs a) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= a.n_elig) return;
+  const int64_t g = a.off + i;
+  if (!merge_nonzero(a.x0, a.cap, g)) return;
+  const double x[3] = {a.x0[g], a.x0[a.cap + g], a.x0[2 * a.cap + g]};
+  const double ri = a.sig[g];
+  const double ext = a.reach * (ri + a.rmax);
+  int64_t c0[3], c1[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    c0[m] = merge_cell(x[m] - ext, a.h);
+    c1[m] = merge_cell(x[m] + ext, a.h);
   }
-  // sources: tiles from this CTA's first target on, split over gridDim.y
-  const int64_t first = blockIdx.x * (int64_t)BLOCK;
-  const int64_t tiles = (a.n - first + BLOCK - 1) / BLOCK;
-  for (int64_t t = blockIdx.y; t < tiles; t += gridDim.y) {
-    const int64_t jb = first + t * BLOCK;
-    __syncthreads();
-    const int64_t j = jb + threadIdx.x;
-    if (j < a.n) {
-      const int64_t g = a.off + j;
-      const bool nz = a.x0[3 * cap + g] != 0.0 || a.x0[4 * cap + g] != 0.0 || a.x0[5 * cap + g] != 0.0;
-      sP[threadIdx.x] = make_double4(a.x0[g], a.x0[cap + g], a.x0[2 * cap + g], nz ? a.sig[g] : CUDART_NAN);
-    } else {
-      sP[threadIdx.x] = make_double4(0.0, 0.0, 0.0, CUDART_NAN);
-    }
-    __syncthreads();
-    if (!vi) continue;
-    const int cnt = (int)min((int64_t)BLOCK, a.n - jb);
-    for (int jj = 0; jj < cnt; ++jj) {
-      const double4 p = sP[jj];
-      const double dx = xi - p.x, dy = yi - p.y, dz = zi - p.z;
-      const double lim = a.reach * (ri + p.w);
-      const double d2 = dx * dx + dy * dy + dz * dz;
-      if (jb + jj > i && d2 < lim * lim) {
-        const double pawan = 0.125 * (ri + p.w);
-        const unsigned long long out = d2 >= pawan * pawan * (1.0 + 1e-12) ? 1ull : 0ull;
-        const unsigned long long k = atomicAdd(a.count, 1ull);
-        if ((int64_t)k < a.max_pairs)
-          a.pairs[k] = ((unsigned long long)i << 32) | ((unsigned long long)(jb + jj) << 1) | out;
+  for (int64_t cx = c0[0]; cx <= c1[0]; ++cx)
+    for (int64_t cy = c0[1]; cy <= c1[1]; ++cy)
+      for (int64_t cz = c0[2]; cz <= c1[2]; ++cz) {
+        const unsigned long long key = merge_cell_key(cx, cy, cz);
+        int64_t lo = 0, hi = a.n;  // first sorted key >= key
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if (a.keys[mid] < key) lo = mid + 1;
+          else hi = mid;
+        }
+        for (int64_t e = lo; e < a.n && a.keys[e] == key; ++e) {
+          const int64_t j = a.idx[e];
+          if (j <= i) continue;
+          const double4 p = a.rec[e];
+          const double dx = x[0] - p.x, dy = x[1] - p.y, dz = x[2] - p.z;
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          const double lim = a.reach * (ri + p.w);
+          if (d2 < lim * lim) {
+            const double pawan = 0.125 * (ri + p.w);
+            const unsigned long long out = d2 >= pawan * pawan * (1.0 + 1e-12) ? 1ull : 0ull;
+            const unsigned long long k = atomicAdd(a.count, 1ull);
+            if ((int64_t)k < a.max_pairs)
+              a.pairs[k] = ((unsigned long long)i << 32) | ((unsigned long long)j << 1) | out;
+          }
+        }
       }
-    }
-  }
 }
 
 // Velocity induced at arbitrary points by particles [lo, hi) with each

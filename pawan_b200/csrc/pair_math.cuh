@@ -168,22 +168,23 @@ __device__ __forceinline__ PairTerms<double> pair_terms(double r2, double s2) {
 //   q    = rb^3 (rb^2 + 2.5) / (4 pi w^2.5 rho^3)           (QSIG)
 //   eta  = 13.125 / (pi sigma^3 w^4.5)                      (ETASIG, the diffusion kernel)
 //   F    = (zeta - 3 q) / rho^2                             (KERNEL)
-// In the 4 pi scaled units of PairTerms, with s = 1/sigma and u = rb^2:
-//   q'  = (u + 2.5) s^3 w^-2.5
-//   F'  = (7.5 w^-3.5 - 3 (u + 2.5) w^-2.5) s^3 / rho^2 = -3 (u + 3.5) s^5 w^-3.5
-//   zd' = 4 pi eta / sigma^2 = 52.5 s^5 w^-4.5
-// The reduced F' is the same function with the 1/rho^2 cancelled by hand, so
-// it has no cancellation as rho -> 0 and every term is finite at rho = 0.  As
-// for the Gaussian kernel, all three terms are zeroed at rho = 0: the self
-// pair (and coincident particles, where PAWAN's QSIG is 0/0) contributes
-// exact zeros; with contracted multiply-adds v_t a_t - v_t a_t would not be.
-// No regime split: all powers of w come from one reciprocal square root.
+// In the 4 pi scaled units of PairTerms, with s2 = sigma^2, r2 = rho^2 and
+// R = r2 + s2 (so that rb^2 + 1 = R / s2 and every power of sigma cancels):
+//   q'   = (r2 + 2.5 s2) R^-2.5
+//   F'   = (7.5 s2^2 R^-3.5 - 3 q') / r2 = -3 (r2 + 3.5 s2) R^-3.5
+//   zd'  = 4 pi eta / s2 = 52.5 s2^2 R^-4.5
+//   zeta = 1.875 / pi s2^2 R^-3.5
+// The reduced F' is PAWAN's (zeta - 3 q)/rho^2 with the 1/rho^2 cancelled by
+// hand, so it has no cancellation as rho -> 0, and all terms come from one
+// reciprocal square root of R, a sum of two positive numbers.  As for the
+// Gaussian kernel, the terms are zeroed at rho = 0: the self pair (and
+// coincident particles, where PAWAN's QSIG is 0/0) contributes exact zeros;
+// with contracted multiply-adds v_t a_t - v_t a_t would not be.
 //
-// FP32: F' carries s^5 w^-3.5, so a relative error e of each reciprocal square
-// root becomes ~12 e in F'.  The hardware approximation's error is a fixed
-// function of its input, so it does not average out over the sum (it left
-// 2e-5 of max |dalpha| on two leapfrogging rings); one Newton step brings each
-// root to about one rounding.
+// FP32: F' carries R^-3.5, so a relative error e of the reciprocal square
+// root becomes 3.5 e.  The hardware approximation's error is a fixed function
+// of its input, so it does not average out over the sum; one Newton step
+// brings the root to about one rounding.
 struct HighOrder {
   static constexpr double kQ0 = 2.5, kF0 = 3.5, kZd = 52.5, kZeta = 7.5;
 };
@@ -196,34 +197,28 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 }
 
 __device__ __forceinline__ PairTerms<float> pair_terms_ho(float r2, float s2) {
-  const float is = rsqrt_nr(s2);
-  const float is2 = is * is;
-  const float is3 = is * is2 * (r2 > 0.0f ? 1.0f : 0.0f);
-  const float u = r2 * is2;
-  const float iw = rsqrt_nr(u + 1.0f);
-  const float iw2 = iw * iw;
-  const float iw5 = iw2 * iw2 * iw;
-  const float iw7 = iw5 * iw2;
+  const float m = r2 > 0.0f ? 1.0f : 0.0f;
+  const float iR = rsqrt_nr(r2 + s2);
+  const float iR2 = iR * iR;
+  const float iR5 = iR2 * iR2 * iR;
+  const float iR7 = iR5 * iR2;
   PairTerms<float> o;
-  o.q = (u + (float)HighOrder::kQ0) * is3 * iw5;
-  o.F = -3.0f * (u + (float)HighOrder::kF0) * (is3 * is2) * iw7;
-  o.zd = (float)HighOrder::kZd * (is3 * is2) * (iw7 * iw2);
+  o.q = fmaf((float)HighOrder::kQ0, s2, r2) * (iR5 * m);
+  o.F = fmaf((float)HighOrder::kF0, s2, r2) * (iR7 * (-3.0f * m));
+  o.zd = ((float)HighOrder::kZd * s2 * s2) * (iR7 * iR2 * m);
   return o;
 }
 
 __device__ __forceinline__ PairTerms<double> pair_terms_ho(double r2, double s2) {
-  const double is = 1.0 / sqrt(s2);
-  const double is2 = is * is;
-  const double is3 = is * is2 * (r2 > 0.0 ? 1.0 : 0.0);
-  const double u = r2 * is2;
-  const double iw = 1.0 / sqrt(u + 1.0);
-  const double iw2 = iw * iw;
-  const double iw5 = iw2 * iw2 * iw;
-  const double iw7 = iw5 * iw2;
+  const double m = r2 > 0.0 ? 1.0 : 0.0;
+  const double iR = 1.0 / sqrt(r2 + s2);
+  const double iR2 = iR * iR;
+  const double iR5 = iR2 * iR2 * iR;
+  const double iR7 = iR5 * iR2;
   PairTerms<double> o;
-  o.q = (u + HighOrder::kQ0) * is3 * iw5;
-  o.F = -3.0 * (u + HighOrder::kF0) * (is3 * is2) * iw7;
-  o.zd = HighOrder::kZd * (is3 * is2) * (iw7 * iw2);
+  o.q = fma(HighOrder::kQ0, s2, r2) * (iR5 * m);
+  o.F = fma(HighOrder::kF0, s2, r2) * (iR7 * (-3.0 * m));
+  o.zd = (HighOrder::kZd * s2 * s2) * (iR7 * iR2 * m);
   return o;
 }
 
