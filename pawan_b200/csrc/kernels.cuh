@@ -161,14 +161,14 @@ struct WarpBox {
 // (hs_t + hs_s) >= kFarU: the squared gap between the boxes is a lower bound
 // of every pair's r^2.  A zero gap (touching or overlapping boxes, coincident
 // particles) is never far.
-__device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s) {
+__device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s, float far_u = kFarU) {
   float d2 = 0.f;
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     const float gap = fmaxf(fmaxf(s.lo[m] - t.hi[m], t.lo[m] - s.hi[m]), 0.f);
     d2 = fmaf(gap, gap, d2);
   }
-  return d2 > 0.f && d2 >= kFarU * (t.hs + s.hs);
+  return d2 > 0.f && d2 >= far_u * (t.hs + s.hs);
 }
 
 // BLOCK threads, TPT targets per thread, TILE sources per shared-memory tile
@@ -182,6 +182,13 @@ __device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s) {
 template <typename T, int BLOCK, int TPT, int CG, int KER>
 __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
   constexpr bool kGauss32 = sizeof(T) == 4 && KER == kGaussian;
+  // Gaussian kernel: tiles whose sources are all far from the warp's targets
+  // take the far limit with no per-pair test (u >= 50 in FP32, u >= 100 in
+  // FP64, where the limit equals the closed form to the precision).  The
+  // boxes are kept in FP32: a pair misjudged by their rounding sits at
+  // u = 100 (1 - 1e-6) or so, where the far limit is still exact in FP64.
+  constexpr bool kTiled = KER == kGaussian;
+  constexpr float kTileFarU = sizeof(T) == 4 ? kFarU : (float)kFarU64;
   // Stretching q (a_t x a_s): summed as alpha_t x (sum q alpha_s) per
   // compensation group, except for the FP32 high-order kernel, which forms
   // a_t x a_s per pair.  Along a vortex tube a_t and the group sum are nearly
@@ -194,6 +201,11 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
   static_assert(TILE % CG == 0, "compensation group must divide the tile");
   __shared__ __align__(16) v4_t<T> sP[2][TILE];
   __shared__ __align__(16) v4_t<T> sQ[2][TILE];
+  // far tiles: n_s = (x_s - ref) x alpha_s, ref the tile's first source (as in
+  // the FP32 far loop, pair_f32.cuh): alpha_s x d = alpha_s x X' + n_s with
+  // X' = x_t - ref, so the velocity is (sum q alpha_s) x X' + sum q n_s and
+  // alpha_t . w = alpha_s . (X' x alpha_t) + n_s . alpha_t
+  __shared__ __align__(16) v4_t<T> sN[kTiled ? TILE : 1];
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -232,10 +244,10 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
 #pragma unroll
       for (int m = 0; m < 3; ++m) at3[k][m] = T(-3) * at[k][m];
     }
-    // FP32: bounding box of this warp's targets and their largest sigma^2/2,
-    // for the per-tile all-far test below
+    // bounding box of this warp's targets and their largest sigma^2/2, for the
+    // per-tile all-far test below
     WarpBox tb;
-    if constexpr (kGauss32) {
+    if constexpr (kTiled) {
       tb.init();
 #pragma unroll
       for (int k = 0; k < TPT; ++k) tb.add(xt[k][0], xt[k][1], xt[k][2], hst[k]);
@@ -262,14 +274,15 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
       cp_async_wait<1>();
       __syncthreads();
 
-      // FP32: every pair of this warp's targets with this tile's sources is
-      // far (u >= 50) when the boxes are at least sqrt(50 (hs_t + hs_s)) apart
-      // in every case; such tiles take the far limit with no per-pair test.
+      // Every pair of this warp's targets with this tile's sources is far
+      // (u >= kTileFarU) when the boxes are at least sqrt(kTileFarU (hs_t +
+      // hs_s)) apart; such tiles take the far limit with no per-pair test.
       // The boxes' distance is a lower bound of every pair's, so a far pair
-      // is never misclassified near; a pair within rounding of u = 50 may take
-      // the far limit, whose dropped terms are below 2e-9 there.
+      // is never misclassified near; a pair within rounding of the threshold
+      // may take the far limit, whose dropped terms are below 2e-9 at u = 50
+      // (FP32) and below double rounding at u = 100 (FP64).
       bool far_tile = false;
-      if constexpr (kGauss32) {
+      if constexpr (kTiled) {
         WarpBox sb_box;
         sb_box.init();
         for (int r = lane; r < TILE; r += 32) {
@@ -277,7 +290,19 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
           sb_box.add(p.x, p.y, p.z, p.w);
         }
         sb_box.reduce();
-        far_tile = all_far(tb, sb_box);
+        far_tile = all_far(tb, sb_box, kTileFarU);
+      }
+      // reference point of far tiles and n_s of the source this thread staged
+      // (far_tile is uniform over the warp, not over the CTA: every thread
+      // stages its n_s, and the barrier below is unconditional)
+      T rx = 0, ry = 0, rz = 0;
+      if constexpr (kTiled) {
+        rx = sP[buf][0].x; ry = sP[buf][0].y; rz = sP[buf][0].z;
+        const v4_t<T> p = sP[buf][tid];
+        const v4_t<T> q = sQ[buf][tid];
+        const T px = p.x - rx, py = p.y - ry, pz = p.z - rz;
+        sN[tid] = make_v4<T>(py * q.z - pz * q.y, pz * q.x - px * q.z, px * q.y - py * q.x, T(0));
+        __syncthreads();
       }
 
 #pragma unroll 1
@@ -289,25 +314,35 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
           for (int m = 0; m < 3; ++m) { sv[k][m] = 0; sd[k][m] = 0; sp[k][m] = 0; sdv[k][m] = 0; }
         }
         if (far_tile) {
+          // B3 = X' x (-3 alpha_t)
+          T b3[TPT][3];
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            const T xr0 = xt[k][0] - rx, xr1 = xt[k][1] - ry, xr2 = xt[k][2] - rz;
+            b3[k][0] = xr1 * at3[k][2] - xr2 * at3[k][1];
+            b3[k][1] = xr2 * at3[k][0] - xr0 * at3[k][2];
+            b3[k][2] = xr0 * at3[k][1] - xr1 * at3[k][0];
+          }
 #pragma unroll 4
           for (int jj = 0; jj < CG; ++jj) {
             const v4_t<T> p = sP[buf][g + jj];
             const v4_t<T> q = sQ[buf][g + jj];
+            const v4_t<T> n = sN[g + jj];
 #pragma unroll
             for (int k = 0; k < TPT; ++k) {
               const T dx = xt[k][0] - p.x, dy = xt[k][1] - p.y, dz = xt[k][2] - p.z;
               const T r2 = dx * dx + dy * dy + dz * dz;
-              // far limit: q' = r^3, F' = -3 r^5 (the -3 is in at3), no diffusion
-              const float ir = fast_rsqrt(r2);
-              const float A = ir * ir;
+              // far limit: q' = r^3, F' = -3 r^5 (the -3 is in at3 and b3), no diffusion
+              T ir;
+              if constexpr (sizeof(T) == 4) ir = fast_rsqrt(r2);
+              else ir = rsqrt(r2);
+              const T A = ir * ir;
               const T qq = A * ir;
-              const T wx = q.y * dz - q.z * dy;
-              const T wy = q.z * dx - q.x * dz;
-              const T wz = q.x * dy - q.y * dx;
-              sv[k][0] += qq * wx; sv[k][1] += qq * wy; sv[k][2] += qq * wz;
-              const T fd = (qq * A) * (at3[k][0] * wx + at3[k][1] * wy + at3[k][2] * wz);
-              sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
               sp[k][0] += qq * q.x; sp[k][1] += qq * q.y; sp[k][2] += qq * q.z;
+              sv[k][0] += qq * n.x; sv[k][1] += qq * n.y; sv[k][2] += qq * n.z;
+              const T fd = (qq * A) * (q.x * b3[k][0] + q.y * b3[k][1] + q.z * b3[k][2] +
+                                       n.x * at3[k][0] + n.y * at3[k][1] + n.z * at3[k][2]);
+              sd[k][0] += fd * dx; sd[k][1] += fd * dy; sd[k][2] += fd * dz;
             }
           }
         } else {
@@ -390,6 +425,14 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
         }
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
+          if (far_tile) {
+            // velocity = (sum q alpha_s) x X' + sum q n_s
+            const T xr0 = xt[k][0] - rx, xr1 = xt[k][1] - ry, xr2 = xt[k][2] - rz;
+            const T n0 = sv[k][0], n1 = sv[k][1], n2 = sv[k][2];
+            sv[k][0] = sp[k][1] * xr2 - sp[k][2] * xr1 + n0;
+            sv[k][1] = sp[k][2] * xr0 - sp[k][0] * xr2 + n1;
+            sv[k][2] = sp[k][0] * xr1 - sp[k][1] * xr0 + n2;
+          }
           // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t)
           T cx, cy, cz;
           if constexpr (kPairCross) {
