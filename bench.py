@@ -28,7 +28,7 @@ host cores with all threads: each step is one RK4 step of a random
 SAMPLE_N-particle subset of the same ring, and the reported steps/s is
 extrapolated to N by the ratio of pair counts.
 
-The `surrogate` object times configuration 5 on rank 0: two coaxial rings of
+The `surrogate` object times the far-field surrogate on rank 0: two coaxial rings of
 4M particles, one RK4 step with the octree far field (quadrupole order,
 sampled direct-sum check of 4096 targets per evaluation) against the plain
 direct-sum RK4 step.

@@ -288,7 +288,7 @@ def test_growing_wake_matches_restatement(gpu, prec):
 
 @pytest.fixture(scope="module")
 def ring1m():
-    """Configuration 2 at full size: 1000 stations x 1000 particles, Gaussian
+    """The 1M-particle ring: 1000 stations x 1000 particles, Gaussian
     cross-section, sigma = 0.02, seed 1."""
     return cases.ring_gaussian()
 
@@ -324,8 +324,8 @@ def test_ring1m_stretching_and_diffusion_sum_to_zero(gpu, ring1m_rates):
     assert tot <= 1e-6 * scale
 
 
-def test_config3_64_uneven_rings_batched_sampled(gpu):
-    """Configuration 3 at full size: 64 independent rings, N log-uniform in
+def test_64_uneven_rings_batched_sampled(gpu):
+    """64 independent rings, N log-uniform in
     [2e3, 2e5] (seed 2), as 64 systems of one context evaluated in one
     persistent launch; 64 seeded targets of the three smallest and three
     largest rings against the FP64 restatement of each ring alone."""
