@@ -152,7 +152,8 @@ class RotorShedder:
     """Synthetic rotor tip-vortex shedder for a growing wake.
 
     ``blades`` tip vortices of a rotor of radius ``radius`` turning by
-    ``dpsi_deg`` per step (Omega = 1, so dt = dpsi in radians).  Each step every
+    ``dpsi_deg`` per step at angular speed ``omega``, so dt = dpsi / omega
+    (dpsi in radians; omega = 1 by default).  Each step every
     blade sheds ``per_blade`` particles spread along the tip-helix segment it
     swept during the step; the helix descends ``pitch`` per revolution.  Each
     particle carries Gamma times its segment length along the helix tangent,
@@ -168,11 +169,12 @@ class RotorShedder:
     core: float = 0.02
     sigma: float = 0.03
     inflow: tuple = (0.0, 0.0, -0.05)
+    omega: float = 1.0
     step_index: int = field(default=0)
 
     @property
     def dt(self) -> float:
-        return math.radians(self.dpsi_deg)
+        return math.radians(self.dpsi_deg) / self.omega
 
     def shed(self) -> Wake:
         """Particles shed during the current step (advances the step counter)."""
