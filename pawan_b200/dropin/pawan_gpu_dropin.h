@@ -12,7 +12,8 @@
  *     IN->integrate(S, IO, true);                              // unchanged
  *
  * __gpu overrides the virtual members of __interaction that carry the hot
- * path (interaction.h:192-241): solve, diagnose, addWake.  Particle data stays
+ * path (interaction.h:192-244): solve, diagnose, addWake, relax, and the
+ * protected influence behind resolve().  Particle data stays
  * authoritative in the host __wake matrices, exactly as in PAWAN; every solve
  * uploads the current positions/strengths and writes the rates back into
  * __wake::_velocity / _retvorcity, so getRates/getStates/setStates/write keep
