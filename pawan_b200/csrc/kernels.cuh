@@ -484,15 +484,16 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
 
 namespace pgpu {
 
-// FP64 Gaussian shapes with one target per thread are held to 128 registers
-// (a few bytes of spill), which fits two 256-thread CTAs per SM instead of
-// one: 3196 ms instead of 3632 ms per evaluation of the 1M ring.  With more
-// targets per thread the same cap spills hundreds of bytes, so those shapes
-// keep the registers they need.
+// FP64 shapes with one target per thread are held to 128 registers (a few
+// bytes of spill), which fits two 256-thread CTAs per SM instead of one: per
+// evaluation of the 1M ring 3196 ms instead of 3632 ms (Gaussian) and
+// 4505 ms instead of 5743 ms (high-order).  With more targets per thread the
+// same cap spills hundreds of bytes, so those shapes keep the registers they
+// need.
 template <typename T, int BLOCK, int TPT, int KER>
 constexpr int pair_min_blocks() {
   return sizeof(T) == 4 && KER == kGaussian ? pair_f32_min_blocks<BLOCK, TPT>()
-         : (sizeof(T) == 8 && KER == kGaussian && TPT == 1) ? (65536 / (BLOCK * 128) > 0 ? 65536 / (BLOCK * 128) : 1)
+         : (sizeof(T) == 8 && TPT == 1) ? (65536 / (BLOCK * 128) > 0 ? 65536 / (BLOCK * 128) : 1)
                                                             : 1;
 }
 
