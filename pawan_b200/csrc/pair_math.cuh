@@ -1,6 +1,7 @@
 // Per-pair regularised Biot-Savart / stretching / diffusion terms of PAWAN's
-// Gaussian vortex-particle kernel, for FP32 (compensated accumulation around
-// it) and FP64.
+// vortex-particle kernels, for FP32 (compensated accumulation around it) and
+// FP64: the Gaussian kernel (below, and the FP32 three-regime form further
+// down) and the high-order algebraic kernel (pair_terms_ho).
 //
 // Reference algorithm (src/interaction/gaussian.h:20-60 and
 // src/interaction/interaction_utils.h:55-105, 344-378, 523-576), per ordered
