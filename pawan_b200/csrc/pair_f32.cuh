@@ -263,7 +263,13 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
               sv[k][0].x += qq * wx; sv[k][1].x += qq * wy; sv[k][2].x += qq * wz;
               const float fd = FF * (at[k][0] * wx + at[k][1] * wy + at[k][2] * wz);
               sd[k][0].x += fd * dx; sd[k][1].x += fd * dy; sd[k][2].x += fd * dz;
-              sp[k][0].x += qq * qx; sp[k][1].x += qq * qy; sp[k][2].x += qq * qz;
+              // near tiles: q (alpha_t x alpha_s) per pair.  Along a filament the
+              // neighbours' strengths are nearly parallel to alpha_t, and
+              // alpha_t x (sum q alpha_s) would keep only the FP32 rounding of
+              // the parallel part (2.3e-5 of max |dalpha| on a rotor tip vortex)
+              sp[k][0].x += qq * (at[k][1] * qz - at[k][2] * qy);
+              sp[k][1].x += qq * (at[k][2] * qx - at[k][0] * qz);
+              sp[k][2].x += qq * (at[k][0] * qy - at[k][1] * qx);
             }
           };
 #pragma unroll 1
@@ -291,10 +297,17 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
             svs[1] = sps[2] * xr0 - sps[0] * xr2 + n1;
             svs[2] = sps[0] * xr1 - sps[1] * xr0 + n2;
           }
-          // da = alpha_t x (sum q alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t)
-          const float ex = at[k][1] * sps[2] - at[k][2] * sps[1] + sds[0] + a.nu2 * sdv[k][0];
-          const float ey = at[k][2] * sps[0] - at[k][0] * sps[2] + sds[1] + a.nu2 * sdv[k][1];
-          const float ez = at[k][0] * sps[1] - at[k][1] * sps[0] + sds[2] + a.nu2 * sdv[k][2];
+          // da = sum q (alpha_t x alpha_s) + sum F (d.c) d + 2 nu sum z (v_t a_s - v_s a_t);
+          // far tiles summed q alpha_s, near tiles q (alpha_t x alpha_s) itself
+          float c0 = sps[0], c1 = sps[1], c2 = sps[2];
+          if (far_tile) {
+            c0 = at[k][1] * sps[2] - at[k][2] * sps[1];
+            c1 = at[k][2] * sps[0] - at[k][0] * sps[2];
+            c2 = at[k][0] * sps[1] - at[k][1] * sps[0];
+          }
+          const float ex = c0 + sds[0] + a.nu2 * sdv[k][0];
+          const float ey = c1 + sds[1] + a.nu2 * sdv[k][1];
+          const float ez = c2 + sds[2] + a.nu2 * sdv[k][2];
           two_sum_acc(vh[k][0], vl[k][0], svs[0]);
           two_sum_acc(vh[k][1], vl[k][1], svs[1]);
           two_sum_acc(vh[k][2], vl[k][2], svs[2]);
