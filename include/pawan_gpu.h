@@ -133,7 +133,8 @@ int pgpu_step(pgpu_ctx *ctx, int scheme, double dt, int32_t nsteps);
  * pgpu_set_target_range: targets [first, first + count) of the system (in
  * the order of its wakes' particles); count < 0 restores all targets.  While
  * any system has a range, pgpu_step and pgpu_diagnose refuse (the state of
- * the other targets is not advanced here), and the surrogate is off.
+ * the other targets is not advanced here; pgpu_diagnose_partial gives this
+ * context's share of the diagnostics), and the surrogate is off.
  * pgpu_stage: stage 0..3 (RK4), 0..2 (RK3) or 0 (Euler) of one step of every
  * system; the last stage finishes the step (and applies vinf).
  * pgpu_records: device pointers to the system's source records, one per
@@ -185,6 +186,32 @@ int pgpu_get_particles(pgpu_ctx *ctx, int32_t wake, double *pos, double *alpha, 
  * with non-zero weight wins, else the previous value is kept. */
 int pgpu_diagnose(pgpu_ctx *ctx, int32_t system, double *out, double *vbi);
 
+/* The two halves of pgpu_diagnose, for a system split over several contexts
+ * by target ranges (no PAWAN counterpart; PAWAN sums on one host,
+ * parallel.cpp:140-401 and interaction.cpp:92-132).
+ *
+ * pgpu_diagnose_partial: PGPU_DIAG_FIELDS FP64 sums per wake of the system
+ * (fields[k * PGPU_DIAG_FIELDS + m] for the k-th wake of the system, in the
+ * order added) over this context's owned targets, every target if it has no
+ * range.  The O(N^2) terms (helicity, kinetic energies, enstrophies) are
+ * summed over the unordered pairs whose lower index is an owned target, so
+ * the sum of the contexts' fields over a partition of the targets is the
+ * whole system's: in FP32C from the source records, which the contexts
+ * share after each exchange; the O(N) terms from the owned FP64 state.
+ * Layout: 0-2 sum alpha, 3-5 sum x x alpha, 6-8 sum x x (x x alpha), 9-10 the
+ * numerator and denominator of Zc, 11-13 the velocity at the origin, 14
+ * helicity, 15-16 pair terms of KE and KEF, 17-18 their self terms, 19-20
+ * pair terms of the enstrophies, 21-22 their self terms.
+ *
+ * pgpu_diagnose_combine (host only, no device work): the 15-value record of
+ * pgpu_diagnose and vbi from fields summed over the contexts (an all-reduce
+ * of nwakes x PGPU_DIAG_FIELDS doubles); zc_prev is the previous Zc, kept if
+ * no wake has weight, and *zc_out (may be NULL) receives the new one. */
+#define PGPU_DIAG_FIELDS 23
+int pgpu_diagnose_partial(pgpu_ctx *ctx, int32_t system, double *fields);
+int pgpu_diagnose_combine(const double *fields, int32_t nwakes, double zc_prev, double *out, double *vbi,
+                          double *zc_out);
+
 /* Replaces: __interaction::getVi (interaction.cpp:453-477) and the airstation
  * loop of getInflow (:399-451): velocity induced at npts points (row-major
  * (npts, 3)) by every particle of a system, using each particle's own radius. */
@@ -209,9 +236,11 @@ int pgpu_pair_kernel_time(pgpu_ctx *ctx, double *ms, int64_t *launches);
 
 /* Ordered pair interactions (self pairs excluded) evaluated by the pair
  * kernel since the last call, and how many of them took the full formula;
- * the rest took the far-field limit (FP32C mode, rho^2 >= 50 sigma^2, where
- * erf rounds to 1 and exp(-rho^2/2sigma^2) < 1.4e-11).  Resets both counts.
- * No PAWAN counterpart (PAWAN has no counters). */
+ * with the Gaussian kernel the rest took the far-field limit (FP32C:
+ * rho^2 >= 50 sigma^2, where erf rounds to 1 and exp(-rho^2/2sigma^2) <
+ * 1.4e-11; FP64: rho^2 >= 100 sigma^2, where the limit equals the closed form
+ * to double rounding).  The high-order kernel counts every pair as full.
+ * Resets both counts.  No PAWAN counterpart (PAWAN has no counters). */
 int pgpu_pair_counts(pgpu_ctx *ctx, int64_t *pairs, int64_t *full_pairs);
 
 /* Kernel launches issued since context creation (all kernels of this library). */
@@ -225,27 +254,60 @@ int pgpu_autotune(pgpu_ctx *ctx, int reps, int *block, int *tpt, double *ms_per_
 /* Number of compiled pair-kernel shapes and their (block, tpt). */
 int pgpu_kernel_shapes(int *block, int *tpt, int max);
 
+/* Autotuning per size class (no PAWAN counterpart: PAWAN's OpenMP loops,
+ * parallel.cpp:14-86, have no tiles to choose).  The systems of a context are
+ * grouped by particle count into classes (class 0: n < 4096; class k >= 1:
+ * 1024 4^k <= n < 1024 4^(k+1)); every compiled shape is timed on each class's
+ * systems alone (`reps` launches after one untimed).  If one shape is within
+ * 2% of each class's fastest, every system uses it (one pair launch per
+ * evaluation); otherwise each class uses its fastest shape, and an evaluation
+ * is one pair launch per distinct shape, each over its classes' systems.
+ * With cache_path set, a class already recorded there for this GPU name,
+ * precision and kernel takes its recorded times instead of being timed, and
+ * newly timed classes are appended, one JSON object per line:
+ *   {"gpu": .., "precision": "fp32c"|"fp64", "kernel": "gaussian"|"highorder",
+ *    "class": k, "nmin": .., "nmax": .., "block": .., "tpt": .., "ms": [one per shape]}
+ * classes[i] (up to max_classes) describes the i-th class present, by
+ * increasing size; *per_class = 1 if the classes launch separately.  The
+ * rates of the current state are recomputed with the chosen launches. */
+typedef struct pgpu_tune_class {
+  int32_t size_class;        /* class index k */
+  int32_t systems;           /* systems of the context in the class */
+  int64_t nmin, nmax;        /* particle counts [nmin, nmax) of the class */
+  int32_t block, tpt;        /* fastest shape of the class */
+  int32_t single_block, single_tpt;  /* the one shape with the least total time over all classes */
+  int32_t from_cache;        /* 1: times read from the cache file */
+  int32_t pad;
+  double ms[8];              /* one pair launch over the class's systems, per shape (pgpu_kernel_shapes order) */
+} pgpu_tune_class;
+int pgpu_autotune_classes(pgpu_ctx *ctx, int reps, const char *cache_path, pgpu_tune_class *classes, int max_classes,
+                          int *nclasses, int *per_class);
+
 /* ---------------------------------------------------------------------------
  * Far-field surrogate (no PAWAN counterpart: PAWAN only has the O(N^2) sum).
  *
  * With the surrogate enabled, every rate evaluation of the context's single
  * system uses an octree: each target leaf's near field (cells closer than
- * near_widths cube widths, or with a particle within 4 sigma_ij of the leaf's)
+ * near_widths cube widths, or with a particle within sqrt(far_u) sigma_ij of the leaf's)
  * is summed exactly with the direct kernel's terms,
  * and farther cells act through their multipole moments (order 0/1/2),
  * optionally corrected by the learned model of pgpu_surrogate_set_mlp.  After
  * every evaluation, check_targets sampled targets are recomputed by the direct
- * sum; if the max-norm relative velocity error exceeds `tolerance`, the
- * evaluation is redone by the direct sum (the surrogate never returns an
- * unchecked result when check_targets > 0). */
+ * sum; if the max-norm relative error of the velocity or of dalpha/dt
+ * exceeds `tolerance`, the evaluation is redone by the direct sum (the
+ * surrogate never returns an unchecked result when check_targets > 0). */
 typedef struct pgpu_surrogate_config {
   int leaf_size;       /* particles per octree leaf, 1..512 (default 256) */
   double near_widths;  /* near field: cells closer than this many cube widths (default 4) */
   int order;           /* far-field expansion: 0 monopole, 1 + dipole, 2 + quadrupole (default) */
   int use_mlp;         /* add the learned correction to the order-1 far field (pgpu_surrogate_set_mlp) */
-  double tolerance;    /* maximum relative velocity error on the sampled targets (default 1e-4) */
+  double tolerance;    /* maximum relative error of the velocity and of dalpha/dt on the sampled targets
+                          (default 1e-4) */
   int check_targets;   /* targets re-checked by the direct sum per evaluation (default 4096, 0 = off) */
   int seed;            /* seed of the sampled targets */
+  double far_u;        /* a far cell's particles are all at rho^2 >= far_u sigma_ij^2 from the leaf's
+                          (default 16, 0 = no test): the expansion is of the singular kernel, and the
+                          Gaussian core it leaves out decays as exp(-far_u / 2) */
 } pgpu_surrogate_config;
 
 typedef struct pgpu_surrogate_stats {
@@ -257,6 +319,7 @@ typedef struct pgpu_surrogate_stats {
   double ms_tree, ms_eval, ms_check, ms_fallback;  /* device time of the last evaluation's phases */
   int64_t cells, leaves;   /* octree of the last evaluation */
   int64_t far_entries, near_entries;  /* interaction-list lengths summed over leaves */
+  double max_err_dalpha;   /* largest sampled dalpha/dt error seen */
 } pgpu_surrogate_stats;
 
 void pgpu_surrogate_config_default(pgpu_surrogate_config *cfg);
@@ -321,6 +384,9 @@ int pgpu_get_stream(pgpu_ctx *ctx, void **stream);
  * counterpart. */
 int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops);
 int pgpu_fp32_peak(int device, double *tflops, double *ms);
+/* The same measurement for the FP64 pipe (DFMA register loop), the bound of
+ * the FP64 mode's pair kernel.  No PAWAN counterpart. */
+int pgpu_fp64_peak(int device, double *tflops);
 
 /* Largest system pgpu_rates_noalloc accepts (its fixed scratch: ~13.6 MB of
  * device memory per GPU, held from library load until process exit). */
@@ -337,8 +403,8 @@ int pgpu_fp32_peak(int device, double *tflops, double *ms);
  * for the legacy default stream); the call does not wait for it.  It never
  * calls cudaMalloc or cudaFree: its intermediates live in one static device
  * array.  The first call on each device looks up that array's address and
- * clears its work counters (a blocking memset), so make it before any stream
- * capture.  Calls share the array: calls that overlap on the GPU (different
+ * clears its work counters (an asynchronous memset on `stream`, ordered
+ * before that call's kernels), so make it before any stream capture.  Calls share the array: calls that overlap on the GPU (different
  * streams, or host threads without ordering) race and must not be issued.
  * n > PGPU_NOALLOC_MAX_N is rejected with PGPU_EINVAL; the reason is in
  * pgpu_noalloc_last_error(). */

@@ -282,3 +282,19 @@ def rel_err(x, ref) -> float:
     num = np.max(np.linalg.norm(x - ref, axis=1))
     den = np.max(np.linalg.norm(ref, axis=1))
     return float(num / den) if den > 0 else float(num)
+
+
+def restate_diagnose_fields(w, row_lo: int, row_hi: int, offsets=None, kernel="gaussian") -> np.ndarray:
+    """Per-wake diagnostic sums over the rows [row_lo, row_hi) in the C ABI's
+    pgpu_diagnose_partial layout, shape (wakes, 23)."""
+    lib = _restate(kernel)
+    if not hasattr(lib, "_fields_bound"):
+        lib.rs_diagnose_fields.argtypes = [C.c_int, _i64p, _dp, _dp, _dp, C.c_int64, C.c_int64, _dp]
+        lib._fields_bound = True
+    if offsets is None:
+        offsets = [0, w.n]
+    off = _c(offsets, np.int64)
+    out = np.zeros((len(offsets) - 1, 23))
+    lib.rs_diagnose_fields(len(offsets) - 1, off.ctypes.data_as(_i64p), _p(_c(w.pos)), _p(_c(w.alpha)),
+                           _p(_c(w.sigma)), int(row_lo), int(row_hi), _p(out))
+    return out

@@ -279,6 +279,75 @@ void rs_getvi(int64_t n, const double *pos, const double *alpha, const double *s
   for (int k = 0; k < 3; ++k) out[k] = u[k];
 }
 
+/* The sums behind rs_diagnose restricted to the rows [row_lo, row_hi) of the
+ * concatenated wakes, per wake, in the field layout of the C ABI's
+ * pgpu_diagnose_partial (23 doubles per wake): 0-2 sum alpha, 3-5 sum
+ * x x alpha, 6-8 sum x x (x x alpha), 9-10 Zc numerator and denominator,
+ * 11-13 velocity at the origin (getVi, interaction.cpp:453-477), 14 helicity,
+ * 15-16 KE and KEF pair terms, 17-18 their self terms, 19-20 enstrophy pair
+ * terms, 21-22 their self terms.  Pair terms of a row i run over every j != i
+ * of the system (ordered pairs, as rs_diagnose), so fields summed over a
+ * partition of the rows give rs_diagnose's totals.  Test code for the
+ * sharded diagnostics. */
+void rs_diagnose_fields(int nw, const int64_t *offsets, const double *pos, const double *alpha,
+                        const double *sigma, int64_t row_lo, int64_t row_hi, double *fields) {
+  const int64_t n = offsets[nw];
+  for (int w = 0; w < nw; ++w) {
+    double *f = fields + 23 * w;
+    for (int m = 0; m < 23; ++m) f[m] = 0.0;
+    const int64_t lo = offsets[w] > row_lo ? offsets[w] : row_lo;
+    const int64_t hi = offsets[w + 1] < row_hi ? offsets[w + 1] : row_hi;
+    for (int64_t i = lo; i < hi; ++i) {
+      const double *x = pos + 3 * i, *a = alpha + 3 * i;
+      double xa[3], xxa[3];
+      cross3(x, a, xa);
+      cross3(x, xa, xxa);
+      for (int k = 0; k < 3; ++k) { f[k] += a[k]; f[3 + k] += xa[k]; f[6 + k] += xxa[k]; }
+      const double om = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+      const double rr = x[0] * x[0] + x[1] * x[1];
+      f[9] += om * x[2] * rr;
+      f[10] += om * rr;
+      const double d0[3] = {-x[0], -x[1], -x[2]};
+      double q0, F0, Z0, eta0, w0[3];
+      kernel_terms(sqrt(rr + x[2] * x[2]), sigma[i], &q0, &F0, &Z0, &eta0);
+      cross3(a, d0, w0);
+      for (int k = 0; k < 3; ++k) f[11 + k] += q0 * w0[k];
+      const double si = sigma[i];
+      const double a2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+      f[17] += a2 / si / 8.0 / M_PI;
+      f[18] += 3.0 * a2 / (si * 16.0) / M_PI;
+      if (g_kernel == 1) {
+        f[21] += 5.0 / M_PI / 2.0 / (si * si * si) * a2;
+        f[22] += 15.0 / M_PI / 8.0 / (si * si * si) * a2;
+      }
+      double h = 0, ke = 0, kef = 0, en = 0, enf = 0;
+#pragma omp parallel for reduction(+ : h, ke, kef, en, enf)
+      for (int64_t j = 0; j < n; ++j) {
+        if (j == i) continue;
+        const double *xj = pos + 3 * j, *aj = alpha + 3 * j;
+        const double d[3] = {xj[0] - x[0], xj[1] - x[1], xj[2] - x[2]};
+        const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        const double s2 = 0.5 * (si * si + sigma[j] * sigma[j]);
+        double q, F, Z, eta, c[3];
+        kernel_terms(sqrt(r2), sqrt(s2), &q, &F, &Z, &eta);
+        cross3(a, aj, c);
+        h += q * (d[0] * c[0] + d[1] * c[1] + d[2] * c[2]);
+        const double aa = a[0] * aj[0] + a[1] * aj[1] + a[2] * aj[2];
+        const double dai = d[0] * a[0] + d[1] * a[1] + d[2] * a[2];
+        const double daj = d[0] * aj[0] + d[1] * aj[1] + d[2] * aj[2];
+        const double den = pow(r2 + s2, 1.5);
+        ke += ((r2 + 2.0 * s2) * aa + dai * daj) / den / 16.0 / M_PI;
+        kef += (r2 + 1.5 * s2) * aa / den / 8.0 / M_PI;
+        double F1, F2, F1F;
+        enst_terms(r2, s2, &F1, &F2, &F1F);
+        en += F1 * aa + F2 * dai * daj;
+        enf += F1F * aa;
+      }
+      f[14] += h; f[15] += ke; f[16] += kef; f[19] += en; f[20] += enf;
+    }
+  }
+}
+
 /* Vorticity field of the listed targets (all if NULL), PAWAN's influence()
  * (interaction.cpp:212-260; INFLUENCE / SELFINFLUENCE, interaction_utils.h:
  * 626-703): k_t = sum_s ZETASIG(rho_ts, sigma_ts) alpha_s over every particle

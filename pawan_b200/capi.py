@@ -34,9 +34,9 @@ EXPORTS = [
     "pgpu_config_default", "pgpu_create", "pgpu_destroy", "pgpu_add_wake", "pgpu_set_particles",
     "pgpu_append_particles", "pgpu_get_num_particles", "pgpu_get_state", "pgpu_set_states_flat",
     "pgpu_get_states_flat", "pgpu_get_rates_flat", "pgpu_solve", "pgpu_get_rates", "pgpu_step",
-    "pgpu_diagnose", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
-    "pgpu_autotune", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
-    "pgpu_fp32_peak", "pgpu_fp32_peaks", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
+    "pgpu_diagnose", "pgpu_diagnose_partial", "pgpu_diagnose_combine", "pgpu_probe", "pgpu_sync", "pgpu_pair_kernel_time", "pgpu_launch_count",
+    "pgpu_autotune", "pgpu_autotune_classes", "pgpu_kernel_shapes", "pgpu_last_error", "pgpu_version", "pgpu_get_stream",
+    "pgpu_fp32_peak", "pgpu_fp32_peaks", "pgpu_fp64_peak", "pgpu_pair_counts", "pgpu_surrogate_config_default", "pgpu_surrogate_enable",
     "pgpu_surrogate_disable", "pgpu_surrogate_get_stats", "pgpu_surrogate_tree", "pgpu_mlp_num_params",
     "pgpu_mlp_create", "pgpu_mlp_destroy", "pgpu_mlp_last_error", "pgpu_mlp_get_params", "pgpu_mlp_set_params",
     "pgpu_mlp_forward", "pgpu_mlp_forward_fused", "pgpu_mlp_gradient", "pgpu_mlp_set_dataset", "pgpu_mlp_add_samples",
@@ -55,7 +55,7 @@ class PgpuConfig(C.Structure):
 
 class SurrogateConfig(C.Structure):
     _fields_ = [("leaf_size", C.c_int), ("near_widths", C.c_double), ("order", C.c_int), ("use_mlp", C.c_int),
-                ("tolerance", C.c_double), ("check_targets", C.c_int), ("seed", C.c_int)]
+                ("tolerance", C.c_double), ("check_targets", C.c_int), ("seed", C.c_int), ("far_u", C.c_double)]
 
 
 class SurrogateStats(C.Structure):
@@ -63,10 +63,16 @@ class SurrogateStats(C.Structure):
                 ("last_err_dalpha", C.c_double), ("max_err_vel", C.c_double), ("ms_tree", C.c_double),
                 ("ms_eval", C.c_double), ("ms_check", C.c_double), ("ms_fallback", C.c_double),
                 ("cells", C.c_int64), ("leaves", C.c_int64), ("far_entries", C.c_int64),
-                ("near_entries", C.c_int64)]
+                ("near_entries", C.c_int64), ("max_err_dalpha", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneClass(C.Structure):
+    _fields_ = [("size_class", C.c_int32), ("systems", C.c_int32), ("nmin", C.c_int64), ("nmax", C.c_int64),
+                ("block", C.c_int32), ("tpt", C.c_int32), ("single_block", C.c_int32), ("single_tpt", C.c_int32),
+                ("from_cache", C.c_int32), ("pad", C.c_int32), ("ms", C.c_double * 8)]
 
 
 class PgpuError(RuntimeError):
@@ -114,17 +120,22 @@ def load(build_if_missing: bool = False):
         "pgpu_get_rates": (C.c_int, [vp, C.c_int32, _dp, _dp]),
         "pgpu_step": (C.c_int, [vp, C.c_int, C.c_double, C.c_int32]),
         "pgpu_diagnose": (C.c_int, [vp, C.c_int32, _dp, _dp]),
+        "pgpu_diagnose_partial": (C.c_int, [vp, C.c_int32, _dp]),
+        "pgpu_diagnose_combine": (C.c_int, [_dp, C.c_int32, C.c_double, _dp, _dp, _dp]),
         "pgpu_probe": (C.c_int, [vp, C.c_int32, C.c_int64, _dp, _dp]),
         "pgpu_sync": (C.c_int, [vp]),
         "pgpu_pair_kernel_time": (C.c_int, [vp, _dp, _i64p]),
         "pgpu_launch_count": (C.c_int64, [vp]),
         "pgpu_autotune": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
         "pgpu_kernel_shapes": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
+        "pgpu_autotune_classes": (C.c_int, [vp, C.c_int, C.c_char_p, C.POINTER(TuneClass), C.c_int,
+                                            C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "pgpu_last_error": (C.c_char_p, [vp]),
         "pgpu_version": (C.c_char_p, []),
         "pgpu_get_stream": (C.c_int, [vp, C.POINTER(vp)]),
         "pgpu_fp32_peak": (C.c_int, [C.c_int, _dp, _dp]),
         "pgpu_fp32_peaks": (C.c_int, [C.c_int, _dp, _dp]),
+        "pgpu_fp64_peak": (C.c_int, [C.c_int, _dp]),
         "pgpu_pair_counts": (C.c_int, [vp, _i64p, _i64p]),
         "pgpu_surrogate_config_default": (None, [C.POINTER(SurrogateConfig)]),
         "pgpu_surrogate_enable": (C.c_int, [vp, C.c_int32, C.POINTER(SurrogateConfig)]),
@@ -194,6 +205,32 @@ def fp32_peak(device: int = 0) -> float:
     if rc != PGPU_OK:
         raise PgpuError(rc, "pgpu_fp32_peak failed")
     return tf.value
+
+
+def fp64_peak(device: int = 0) -> float:
+    """Measured FP64 FMA throughput of the device in TFLOP/s (DFMA register loop)."""
+    lib = load()
+    tf = C.c_double()
+    rc = lib.pgpu_fp64_peak(device, C.byref(tf))
+    if rc != PGPU_OK:
+        raise PgpuError(rc, "pgpu_fp64_peak failed")
+    return tf.value
+
+
+DIAG_FIELDS = 23  # PGPU_DIAG_FIELDS
+
+
+def diagnose_combine(fields, zc_prev: float = 0.0):
+    """pgpu_diagnose_combine (host only): the 15-value diagnostics record, vbi
+    and the new Zc from per-wake fields (wakes x DIAG_FIELDS) summed over the
+    contexts that share a system."""
+    lib = load()
+    f = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1, DIAG_FIELDS)
+    out, vbi, zc = np.zeros(15), np.zeros(3), C.c_double()
+    rc = lib.pgpu_diagnose_combine(_p(f), f.shape[0], float(zc_prev), _p(out), _p(vbi), C.byref(zc))
+    if rc != PGPU_OK:
+        raise PgpuError(rc, "pgpu_diagnose_combine failed")
+    return out, vbi, zc.value
 
 
 NOALLOC_MAX_N = 32768  # PGPU_NOALLOC_MAX_N
@@ -347,6 +384,14 @@ class Context:
         self._ck(self.lib.pgpu_diagnose(self.h, system, _p(out), _p(vbi)))
         return out, vbi
 
+    def diagnose_partial(self, system: int = 0) -> np.ndarray:
+        """pgpu_diagnose_partial: this context's share of the diagnostic sums
+        (its owned targets), one row of DIAG_FIELDS per wake of the system."""
+        nw = sum(1 for s in self.wake_system if s == system)
+        f = np.zeros((nw, DIAG_FIELDS))
+        self._ck(self.lib.pgpu_diagnose_partial(self.h, system, _p(f)))
+        return f
+
     def probe(self, pts, system: int = 0) -> np.ndarray:
         pts = _c(pts).reshape(-1, 3)
         vel = np.zeros_like(pts)
@@ -427,6 +472,26 @@ class Context:
         self._ck(self.lib.pgpu_autotune(self.h, reps, C.byref(b), C.byref(t), _p(ms)))
         shapes = kernel_shapes()
         return (b.value, t.value), {shapes[i]: float(ms[i]) for i in range(len(shapes))}
+
+    def autotune_classes(self, reps: int = 2, cache: str | None = None) -> dict:
+        """pgpu_autotune_classes: shapes per size class of the systems.
+        Returns {"per_class": bool, "classes": [...]}, one dict per class with
+        its particle range, systems, fastest shape, the single shape with the
+        least total time, whether the times came from `cache`, and the time of
+        one launch per shape."""
+        out = (TuneClass * 32)()
+        k, per = C.c_int(), C.c_int()
+        self._ck(self.lib.pgpu_autotune_classes(self.h, reps, cache.encode() if cache else None, out, 32,
+                                                C.byref(k), C.byref(per)))
+        shapes = kernel_shapes()
+        classes = []
+        for i in range(k.value):
+            o = out[i]
+            classes.append({"class": o.size_class, "nmin": o.nmin, "nmax": o.nmax, "systems": o.systems,
+                            "block": o.block, "tpt": o.tpt, "single_block": o.single_block,
+                            "single_tpt": o.single_tpt, "from_cache": bool(o.from_cache),
+                            "ms": {f"{b}x{t}": float(o.ms[j]) for j, (b, t) in enumerate(shapes)}})
+        return {"per_class": bool(per.value), "classes": classes}
 
     # ------------------------------------------------------------ PAWAN flat state vector
     def set_states_flat(self, state, maxn):

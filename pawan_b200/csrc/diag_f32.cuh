@@ -37,14 +37,14 @@ __device__ __forceinline__ void diag_body_f32(const DiagArgs<float> &a) {
     const int64_t local = item - pe.item_start;
     const int64_t tile = local / a.nch;
     const int c = (int)(local - tile * a.nch);
-    const int64_t tend = pe.off + pe.n;
-    const int64_t tlo = pe.off + tile * BLOCK;  // first target of the tile
+    const int64_t tend = pe.off + pe.toff + pe.tn;   // end of the (owned) targets
+    const int64_t tlo = pe.off + pe.toff + tile * BLOCK;  // first target of the tile
     const int64_t t = min(tlo + tid, tend - 1);
     const bool valid = tlo + tid < tend;
     // sources above the tile's first target only (s > t is tested per pair
-    // while a tile can still hold s <= t)
+    // while a tile can still hold s <= t), up to the end of the system
     const int64_t s0 = max(pe.off + (int64_t)c * pe.chunk, tlo);
-    const int64_t s1 = min(pe.off + (int64_t)c * pe.chunk + pe.chunk, tend);
+    const int64_t s1 = min(pe.off + (int64_t)c * pe.chunk + pe.chunk, pe.off + pe.n);
     const float4 pt = a.P[t], qt = a.Q[t];
     const float h50 = kFarU * pt.w;
     const float2 X0 = dup2(pt.x), X1 = dup2(pt.y), X2 = dup2(pt.z), HT = dup2(pt.w);

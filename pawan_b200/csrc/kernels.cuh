@@ -62,7 +62,17 @@ template <typename T> struct PairArgs {
   T nu2;  // 2 nu
   unsigned int *counters;  // [0] next item, [1] finished CTAs
   unsigned long long *nfull;  // accumulated count of full-formula pairs
+  // Bounding boxes of the source records in blocks of kBoxGran slots
+  // (box_kernel): box[2b] = (min x, min y, min z, max sigma^2/2), box[2b+1] =
+  // (max x, max y, max z, 0) over the particles of slots [kBoxGran b,
+  // kBoxGran (b + 1)).  Systems start at multiples of kBoxGran, so every
+  // source tile is a run of whole blocks.  nullptr: the FP32 kernel reduces
+  // each tile's box itself.
+  const float4 *box = nullptr;
 };
+
+// Slots per precomputed source box (divides every pair-kernel tile).
+constexpr int kBoxGran = 64;
 
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -181,7 +191,6 @@ __device__ __forceinline__ bool all_far(const WarpBox &t, const WarpBox &s, floa
 // pair_body_f32 (pair_f32.cuh), the same decomposition with packed FP32.
 template <typename T, int BLOCK, int TPT, int CG, int KER>
 __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
-  constexpr bool kGauss32 = sizeof(T) == 4 && KER == kGaussian;
   // Gaussian kernel: tiles whose sources are all far from the warp's targets
   // take the far limit with no per-pair test (u >= 50 in FP32, u >= 100 in
   // FP64, where the limit equals the closed form to the precision).  The
@@ -401,6 +410,7 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
                   sdv[k][0] += pt.zd * (vt[k] * q.x - q.w * at[k][0]);
                   sdv[k][1] += pt.zd * (vt[k] * q.y - q.w * at[k][1]);
                   sdv[k][2] += pt.zd * (vt[k] * q.z - q.w * at[k][2]);
+                  if constexpr (KER == kGaussian) ++nfull;
                 }
               }
             }
@@ -457,7 +467,7 @@ __device__ __forceinline__ void pair_body_generic(const PairArgs<T> &a) {
       buf ^= 1;
     }
     cp_async_wait<0>();
-    if constexpr (kGauss32) {
+    if constexpr (KER == kGaussian) {
       const unsigned wsum = __reduce_add_sync(0xffffffffu, nfull);
       if ((tid & 31) == 0 && wsum) atomicAdd(a.nfull, (unsigned long long)wsum);
       nfull = 0;
@@ -499,8 +509,9 @@ constexpr int pair_min_blocks() {
 
 template <typename T, int BLOCK, int TPT, int CG, int KER = kGaussian>
 __global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT, KER>())) pair_kernel(PairArgs<T> a) {
-  if constexpr (sizeof(T) == 4 && KER == kGaussian) pair_body_f32<BLOCK, TPT, CG>(a);
-  else pair_body_generic<T, BLOCK, TPT, CG, KER>(a);
+  constexpr int kCG = CG < BLOCK ? CG : BLOCK;  // a group never spans more than one tile
+  if constexpr (sizeof(T) == 4 && KER == kGaussian) pair_body_f32<BLOCK, TPT, kCG>(a);
+  else pair_body_generic<T, BLOCK, TPT, kCG, KER>(a);
 }
 
 // ---------------------------------------------------------------- stage kernel
@@ -534,6 +545,37 @@ __device__ __forceinline__ int find_sys(const int64_t *off, int nsys, int64_t i)
     else hi = mid - 1;
   }
   return lo;
+}
+
+// Source boxes for the FP32 pair kernel's per-tile all-far test (PairArgs::
+// box): one warp per block of kBoxGran slots, over the particles of its
+// system (slots past a system's particle count are left out; a block with
+// none gets an empty box).  O(N) over the FP32 records, run before every pair
+// launch, so appended particles and exchanged records are always covered.
+static __global__ void __launch_bounds__(256) box_kernel(const float4 *P, const int64_t *sys_off, const int64_t *sys_n,
+                                                  int nsys, int64_t cap, int64_t nblocks, float4 *box) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t b = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); b < nblocks; b += warps) {
+    const int64_t s0 = b * kBoxGran;
+    const int si = find_sys(sys_off, nsys, s0);
+    const int64_t end = min(sys_off[si] + sys_n[si], cap);
+    WarpBox w;
+    w.init();
+#pragma unroll
+    for (int k = 0; k < kBoxGran / 32; ++k) {
+      const int64_t j = s0 + lane + 32 * k;
+      if (j < end) {
+        const float4 p = P[j];
+        w.add(p.x, p.y, p.z, p.w);
+      }
+    }
+    w.reduce();
+    if (lane == 0) {
+      box[2 * b] = make_float4(w.lo[0], w.lo[1], w.lo[2], w.hs);
+      box[2 * b + 1] = make_float4(w.hi[0], w.hi[1], w.hi[2], 0.f);
+    }
+  }
 }
 
 template <typename T>
@@ -688,14 +730,14 @@ __device__ __forceinline__ void diag_body_generic(const DiagArgs<T> &a) {
     const int64_t local = item - pe.item_start;
     const int64_t tile = local / a.nch;
     const int c = (int)(local - tile * a.nch);
-    const int64_t tend = pe.off + pe.n;
-    const int64_t tlo = pe.off + tile * BLOCK;  // first target of the tile
+    const int64_t tend = pe.off + pe.toff + pe.tn;   // end of the (owned) targets
+    const int64_t tlo = pe.off + pe.toff + tile * BLOCK;  // first target of the tile
     const int64_t t = min(tlo + tid, tend - 1);
     const bool valid = tlo + tid < tend;
     // sources above the tile's first target only (s > t is tested per pair
-    // while a tile can still hold s <= t)
+    // while a tile can still hold s <= t), up to the end of the system
     const int64_t s0 = max(pe.off + (int64_t)c * pe.chunk, tlo);
-    const int64_t s1 = min(pe.off + (int64_t)c * pe.chunk + pe.chunk, tend);
+    const int64_t s1 = min(pe.off + (int64_t)c * pe.chunk + pe.chunk, pe.off + pe.n);
     const v4_t<T> pt = a.P[t], qt = a.Q[t];
     const T h50 = T(kFarU) * pt.w;
     double h = 0, ke = 0, kef = 0, en = 0, enf = 0;
@@ -1157,6 +1199,24 @@ static __global__ void __launch_bounds__(256) ffma2_peak_kernel(float *out, int 
 #pragma unroll
   for (int k = 0; k < kFfmaChains / 2; ++k) s += x[k].x + x[k].y;
   if (s == -1.2345e30f) *out = s;
+}
+
+// The same probe for the FP64 pipe (DFMA), the bound of the FP64 mode's pair
+// kernel.
+static __global__ void __launch_bounds__(256) dfma_peak_kernel(float *out, int iters, double a, double b) {
+  double x[kFfmaChains];
+#pragma unroll
+  for (int k = 0; k < kFfmaChains; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; i += 4) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int k = 0; k < kFfmaChains; ++k) x[k] = fma(x[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kFfmaChains; ++k) s += x[k];
+  if (s == -1.2345e300) *out = (float)s;
 }
 
 }  // namespace pgpu

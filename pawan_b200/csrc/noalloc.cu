@@ -17,8 +17,9 @@
 // In host code the array's name is only a host-side stand-in, not a device
 // address.  So, once per device and with that device current, the first call
 // asks the runtime for the array's device address (cudaGetSymbolAddress) and
-// clears the work counters.  That first call should therefore come before any
-// stream capture on the device.
+// clears the work counters with an asynchronous memset on the caller's
+// stream, ordered before that call's kernels.  That first call should
+// therefore come before any stream capture on the device.
 //
 // All calls share the one array and it keeps the last call's contents: every
 // call rewrites all it reads.  Calls that overlap on the GPU (on different
@@ -107,7 +108,7 @@ __global__ void noalloc_reduce_kernel(const double *partial, int nch, int64_t n,
 
 // Device address of the scratch array for the current device (set up on the
 // first call for that device).
-int scratch_for_current_device(unsigned char **out, int *grid) {
+int scratch_for_current_device(cudaStream_t st, unsigned char **out, int *grid) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return noalloc_fail(PGPU_ECUDA, "cudaGetDevice failed");
   if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(PGPU_EINVAL, "device %lld is beyond the %lld supported", dev, kMaxDevices);
@@ -120,7 +121,9 @@ int scratch_for_current_device(unsigned char **out, int *grid) {
     // The pair kernel's work counters must start at zero; after that it resets
     // them itself at the end of every launch.  Nothing else needs clearing:
     // each call rewrites the records, the plan and every partial it reads.
-    if (cudaMemset(base + kOffCounters, 0, 256) != cudaSuccess)
+    // The clear goes on the caller's stream, so it is ordered before this
+    // call's pair kernel even on a non-blocking stream.
+    if (cudaMemsetAsync(base + kOffCounters, 0, 256, st) != cudaSuccess)
       return noalloc_fail(PGPU_ECUDA, "clearing the work counters failed");
     int sms = 0, nb = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -145,11 +148,11 @@ extern "C" int pgpu_rates_noalloc(const double *pos, const double *alpha, const 
                         (long long)kNoAllocMaxN);
   if (n == 0) return PGPU_OK;
   if (!pos || !alpha || !sigma || !vol || !vel || !dalpha) return noalloc_fail(PGPU_EINVAL, "null device array");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   unsigned char *base = nullptr;
   int grid = 0;
-  int r = scratch_for_current_device(&base, &grid);
+  int r = scratch_for_current_device(st, &base, &grid);
   if (r) return r;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   float4 *P = reinterpret_cast<float4 *>(base + kOffP);
   float4 *Q = reinterpret_cast<float4 *>(base + kOffQ);
   double *partial = reinterpret_cast<double *>(base + kOffPartial);

@@ -153,12 +153,26 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
       // limit, whose dropped terms are below 2e-9 there.
       WarpBox sbox;
       sbox.init();
-      for (int r = lane; r < NPR; r += 32) {
-        const float4 u = sP[buf][2 * r], v = sP[buf][2 * r + 1];
-        sbox.add(u.x, u.z, v.x, v.z);
-        sbox.add(u.y, u.w, v.y, v.w);
+      if (a.box) {
+        // the tile's blocks of precomputed boxes (the same address in every
+        // lane: one broadcast load each)
+#pragma unroll
+        for (int k = 0; k < TILE / kBoxGran; ++k) {
+          const int64_t b = sb / kBoxGran + k;
+          const float4 lo = __ldg(a.box + 2 * b), hi = __ldg(a.box + 2 * b + 1);
+          sbox.lo[0] = fminf(sbox.lo[0], lo.x); sbox.lo[1] = fminf(sbox.lo[1], lo.y);
+          sbox.lo[2] = fminf(sbox.lo[2], lo.z); sbox.hs = fmaxf(sbox.hs, lo.w);
+          sbox.hi[0] = fmaxf(sbox.hi[0], hi.x); sbox.hi[1] = fmaxf(sbox.hi[1], hi.y);
+          sbox.hi[2] = fmaxf(sbox.hi[2], hi.z);
+        }
+      } else {
+        for (int r = lane; r < NPR; r += 32) {
+          const float4 u = sP[buf][2 * r], v = sP[buf][2 * r + 1];
+          sbox.add(u.x, u.z, v.x, v.z);
+          sbox.add(u.y, u.w, v.y, v.w);
+        }
+        sbox.reduce();
       }
-      sbox.reduce();
       const bool far_tile = all_far(tb, sbox);
 
 #pragma unroll 1

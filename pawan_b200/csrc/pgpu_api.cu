@@ -38,6 +38,7 @@ using namespace pgpu;
 namespace {
 
 constexpr int kCG = kPairCG;
+static_assert(kDiagFields == PGPU_DIAG_FIELDS, "the diagnostic field layout of the header");
 
 struct Shape { int block, tpt; };
 // Compiled pair-kernel shapes (the autotuner chooses among these).
@@ -96,10 +97,17 @@ struct pgpu_ctx {
   size_t d_merge_tmp_bytes = 0;
   unsigned int *d_counters = nullptr;
   unsigned long long *d_nfull = nullptr;
+  float4 *d_box = nullptr;  // FP32 source boxes per kBoxGran slots (box_kernel), FP32C Gaussian contexts
   int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
   int *d_flag = nullptr;
   int diag_blocks = 0;
   int shape = 2;  // (256, 1): the fastest shape at 1M particles before autotuning
+  // Shapes per system chosen by pgpu_autotune_classes (empty: `shape` for
+  // every system).  Each distinct shape in `groups` (ascending) is one pair
+  // launch per evaluation over the systems that use it, with its own plan at
+  // d_plan + g (nsys + 1).
+  std::vector<int> sys_shape;
+  std::vector<int> groups;
   int grid[kNumShapes] = {0};
   int nch = 1;
   bool plan_dirty = true;
@@ -109,7 +117,7 @@ struct pgpu_ctx {
   double pair_ms = 0.0;
   int64_t pair_launches = 0;
   int64_t launches = 0;
-  std::map<std::tuple<int, double, int, int, bool>, cudaGraphExec_t> graphs;  // (scheme, dt, shape, nch, timing)
+  std::map<std::tuple<int, double, int, int, bool>, cudaGraphExec_t> graphs;  // (scheme, dt, launch layout, nch, timing)
   std::vector<cudaGraph_t> graph_defs;
   std::string err;
   SurrogateState *sur = nullptr;  // far-field surrogate of the single system, when enabled
@@ -147,6 +155,13 @@ int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
   } while (0)
 
 bool fp64(const pgpu_ctx *c) { return c->cfg.precision == PGPU_FP64; }
+// The FP32C Gaussian pair kernel tests whole source tiles against boxes
+// precomputed per kBoxGran slots (box_kernel) before each launch.
+bool uses_boxes(const pgpu_ctx *c) { return !fp64(c) && c->cfg.kernel == PGPU_KERNEL_GAUSSIAN; }
+// Boxes cover every slot plus one largest tile (256 slots) past the last:
+// the last tile of the last system may end beyond `cap`, and those blocks
+// hold empty boxes.
+int64_t box_blocks(const pgpu_ctx *c) { return (c->cap + kBoxGran - 1) / kBoxGran + 256 / kBoxGran; }
 size_t rec_bytes(const pgpu_ctx *c) { return fp64(c) ? sizeof(double4) : sizeof(float4); }
 
 int64_t sys_n(const pgpu_ctx *c, int s) {
@@ -183,6 +198,9 @@ int freeze(pgpu_ctx *c) {
   if (c->wakes.empty()) return fail(c, PGPU_EINVAL, "no wakes were added");
   int64_t off = 0;
   for (auto &S : c->sys) {
+    // systems start at multiples of kBoxGran slots, so every source tile of
+    // the pair kernel is a run of whole precomputed boxes
+    off = (off + kBoxGran - 1) / kBoxGran * kBoxGran;
     S.off = off;
     for (int w : S.wakes) {
       c->wakes[w].off = off;
@@ -214,11 +232,12 @@ int freeze(pgpu_ctx *c) {
   if ((r = alloc((void **)&c->d_sysoff, (ns + 1) * sizeof(int64_t)))) return r;
   if ((r = alloc((void **)&c->d_sysn, ns * sizeof(int64_t)))) return r;
   if ((r = alloc((void **)&c->d_syst, 2 * ns * sizeof(int64_t)))) return r;
-  if ((r = alloc((void **)&c->d_plan, (ns + 1) * sizeof(PlanEntry)))) return r;
+  if ((r = alloc((void **)&c->d_plan, (size_t)kNumShapes * (ns + 1) * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_plan_diag, 2 * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_plan_field, (ns + 1) * sizeof(PlanEntry)))) return r;
   if ((r = alloc((void **)&c->d_counters, 4 * sizeof(unsigned int)))) return r;
   if ((r = alloc((void **)&c->d_nfull, sizeof(unsigned long long)))) return r;
+  if (uses_boxes(c) && (r = alloc((void **)&c->d_box, 2 * box_blocks(c) * sizeof(float4)))) return r;
   if ((r = alloc((void **)&c->d_flag, sizeof(int)))) return r;
   c->diag_blocks = 2 * c->sms;
   if ((r = alloc((void **)&c->d_diag, (size_t)c->diag_blocks * kDiagFields * sizeof(double)))) return r;
@@ -291,27 +310,78 @@ std::vector<PlanEntry> build_plan(const pgpu_ctx *c, const std::vector<int> &sys
   return plan;
 }
 
-int choose_nch(const pgpu_ctx *c, int shape) {
+// Source chunks per system for one pair launch of `shape` over `systems`:
+// enough work items for >= 24 per resident CTA, which keeps the tail of the
+// persistent launch below ~2%.
+int choose_nch_for(const pgpu_ctx *c, int shape, const std::vector<int> &systems) {
   if (c->cfg.chunks > 0) return std::min(c->cfg.chunks, kMaxChunks);
   const int64_t TT = (int64_t)kShapes[shape].block * kShapes[shape].tpt;
   int64_t tiles = 0;
-  for (size_t s = 0; s < c->sys.size(); ++s) tiles += ceil_div(owned(c, (int)s).second, TT);
+  for (int s : systems) tiles += ceil_div(owned(c, s).second, TT);
   if (tiles <= 0) return 1;
   const int64_t want = 24LL * c->grid[shape];
   return (int)std::max<int64_t>(1, std::min<int64_t>(kMaxChunks, ceil_div(want, tiles)));
+}
+
+std::vector<int> all_systems(const pgpu_ctx *c) {
+  std::vector<int> all(c->sys.size());
+  for (size_t s = 0; s < all.size(); ++s) all[s] = (int)s;
+  return all;
+}
+
+int choose_nch(const pgpu_ctx *c, int shape) { return choose_nch_for(c, shape, all_systems(c)); }
+
+// Systems that launch with the g-th group's shape.
+std::vector<int> group_systems(const pgpu_ctx *c, int g) {
+  std::vector<int> out;
+  for (size_t s = 0; s < c->sys.size(); ++s)
+    if (c->sys_shape[s] == c->groups[g]) out.push_back((int)s);
+  return out;
+}
+
+// Graph key part that fixes the launch sequence of one evaluation: the single
+// shape, or the set of group shapes.
+int launch_layout(const pgpu_ctx *c) {
+  if (c->groups.empty()) return c->shape;
+  int mask = 0;
+  for (int g : c->groups) mask |= 1 << g;
+  return 1000 + mask;
 }
 
 int upload_plan(pgpu_ctx *c) {
   if (!c->plan_dirty) return PGPU_OK;
   int r = check_contiguous(c);
   if (r) return r;
-  // the surrogate writes one chunk of rates per evaluation
-  c->nch = c->sur ? 1 : choose_nch(c, c->shape);
-  std::vector<int> all(c->sys.size());
-  for (size_t s = 0; s < all.size(); ++s) all[s] = (int)s;
-  std::vector<PlanEntry> plan = build_plan(c, all, c->shape, c->nch);
-  // Unused tail entries keep the sentinel item_start so the device search is bounded.
-  plan.resize(c->sys.size() + 1, plan.back());
+  const size_t ns = c->sys.size();
+  c->groups.clear();
+  if (!c->sur && c->sys_shape.size() == ns) {
+    for (int sh : c->sys_shape)
+      if (std::find(c->groups.begin(), c->groups.end(), sh) == c->groups.end()) c->groups.push_back(sh);
+    std::sort(c->groups.begin(), c->groups.end());
+    if (c->groups.size() == 1) {  // one shape after all: the single-launch path
+      c->shape = c->groups[0];
+      c->groups.clear();
+    }
+  }
+  std::vector<PlanEntry> plan;
+  if (c->groups.empty()) {
+    // the surrogate writes one chunk of rates per evaluation
+    c->nch = c->sur ? 1 : choose_nch(c, c->shape);
+    plan = build_plan(c, all_systems(c), c->shape, c->nch);
+    // Unused tail entries keep the sentinel item_start so the device search is bounded.
+    plan.resize(ns + 1, plan.back());
+  } else {
+    // one chunk count for every group (the stage kernel sums nch chunks of
+    // every particle): the largest any group's launch wants
+    c->nch = 1;
+    for (size_t g = 0; g < c->groups.size(); ++g)
+      c->nch = std::max(c->nch, choose_nch_for(c, c->groups[g], group_systems(c, (int)g)));
+    for (size_t g = 0; g < c->groups.size(); ++g) {
+      std::vector<PlanEntry> p = build_plan(c, group_systems(c, (int)g), c->groups[g], c->nch);
+      p.resize(ns + 1, p.back());
+      plan.insert(plan.end(), p.begin(), p.end());
+    }
+  }
   std::vector<int64_t> off(c->sys.size() + 1), n(c->sys.size());
   for (size_t s = 0; s < c->sys.size(); ++s) { off[s] = c->sys[s].off; n[s] = sys_n(c, (int)s); }
   off[c->sys.size()] = c->cap;
@@ -340,6 +410,21 @@ void account_pairs(pgpu_ctx *c, int launches) {
   }
 }
 
+int launch_boxes(pgpu_ctx *c) {
+  const int64_t nb = box_blocks(c);
+  const int grid = (int)std::min<int64_t>(ceil_div(nb, 8), 16LL * c->sms);  // 8 warps per CTA, one per block
+  box_kernel<<<grid, 256, 0, c->st>>>(static_cast<const float4 *>(c->P), c->d_sysoff, c->d_sysn, (int)c->sys.size(),
+                                      c->cap, nb, c->d_box);
+  CK(cudaGetLastError());
+  c->launches++;
+  return PGPU_OK;
+}
+
+// Kernel launches of one rate evaluation by the direct sum.
+int64_t eval_launches(const pgpu_ctx *c) {
+  return (int64_t)std::max<size_t>(1, c->groups.size()) + (uses_boxes(c) ? 1 : 0);
+}
+
 template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   PairArgs<T> a;
   a.P = static_cast<const v4_t<T> *>(c->P);
@@ -352,14 +437,32 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
   a.nu2 = (T)(2.0 * c->cfg.nu);
   a.counters = c->d_counters;
   a.nfull = c->d_nfull;
+  if (uses_boxes(c)) {
+    // source boxes of the current records, ahead of (and outside the timing of) the pair launch
+    int r = launch_boxes(c);
+    if (r) return r;
+    a.box = c->d_box;
+  }
   // Inside stream capture an event record only becomes a timestamp node of
   // the graph when it is marked external.
   const unsigned flags = c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][0], c->st, flags));
-  pair_fn<T>(c->shape, c->cfg.kernel)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
-  CK(cudaGetLastError());
+  if (c->groups.empty()) {
+    pair_fn<T>(c->shape, c->cfg.kernel)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
+    CK(cudaGetLastError());
+    c->launches++;
+  } else {
+    // one launch per group shape, each over its own plan; the launches share
+    // the work counters, which each resets when its last CTA leaves
+    for (size_t g = 0; g < c->groups.size(); ++g) {
+      const int sh = c->groups[g];
+      a.plan = c->d_plan + g * (c->sys.size() + 1);
+      pair_fn<T>(sh, c->cfg.kernel)<<<c->grid[sh], kShapes[sh].block, 0, c->st>>>(a);
+      CK(cudaGetLastError());
+      c->launches++;
+    }
+  }
   if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][1], c->st, flags));
-  c->launches++;
   if (!c->capturing) account_pairs(c, 1);
   return PGPU_OK;
 }
@@ -510,7 +613,7 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
                   c->d_sysoff, c->d_sysn, c->d_syst, c->d_plan, c->d_plan_diag, c->d_plan_field, c->d_field,
-                  c->d_counters, c->d_nfull, c->d_flag, c->d_merge, c->d_merge_tmp};
+                  c->d_counters, c->d_nfull, c->d_flag, c->d_merge, c->d_merge_tmp, c->d_box};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
@@ -705,7 +808,7 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
     }
     return PGPU_OK;
   }
-  auto key = std::make_tuple(scheme, dt, c->shape, c->nch, c->timing);
+  auto key = std::make_tuple(scheme, dt, launch_layout(c), c->nch, c->timing);
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
@@ -725,25 +828,29 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
   }
   for (int i = 0; i < nsteps; ++i) {
     CK(cudaGraphLaunch(it->second, c->st));
-    c->launches += 2 * ns;
+    c->launches += (1 + eval_launches(c)) * ns;
     account_pairs(c, ns);
     if ((r = collect_timing(c, ns))) return r;
   }
   return PGPU_OK;
 }
 
-int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
-  NvtxRange nvtx("pgpu_diagnose");
-  if (!c || !out) return PGPU_EINVAL;
+int pgpu_diagnose_partial(pgpu_ctx *c, int32_t system, double *fields) {
+  NvtxRange nvtx("pgpu_diagnose_partial");
+  if (!c || !fields) return PGPU_EINVAL;
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
-  if (restricted(c)) return fail(c, PGPU_EINVAL, "diagnostics need the whole state: clear the target ranges first");
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   int r = check_contiguous(c);
   if (r) return r;
   const int shape = 2;  // 256-thread tiles for the diagnostic pair sums
   const int block = 256;
-  const int nch = std::max(1, std::min(kMaxChunks, (int)ceil_div(8LL * c->sms, std::max<int64_t>(1, ceil_div(sys_n(c, system), block)))));
-  std::vector<PlanEntry> plan = build_plan(c, {system}, shape, nch, false);
+  const auto own = owned(c, system);
+  const int64_t row_lo = c->sys[system].off + own.first, row_hi = row_lo + own.second;
+  const int nch = std::max(1, std::min(kMaxChunks, (int)ceil_div(8LL * c->sms, std::max<int64_t>(1, ceil_div(own.second, block)))));
+  // rows: the owned targets (all of them without a target range); each
+  // unordered pair is summed from its lower index, so the ranks' row ranges
+  // together cover every pair once
+  std::vector<PlanEntry> plan = build_plan(c, {system}, shape, nch, true);
   CK(cudaMemcpyAsync(c->d_plan_diag, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   const bool quad = plan.size() > 1;
@@ -766,26 +873,39 @@ int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
     CK(cudaGetLastError());
     c->launches++;
   }
-  double f[kDiagFields] = {0};
-  double zc = c->sys[system].zc;
   std::vector<double> h((size_t)c->diag_blocks * kDiagFields);
-  for (int w : c->sys[system].wakes) {
-    const WakeRec &W = c->wakes[w];
-    if (W.n == 0) continue;
-    const int grid = (int)std::min<int64_t>(ceil_div(W.n, 256), c->diag_blocks);
-    diag_wake_kernel<<<grid, 256, 0, c->st>>>(c->x0, c->sig, c->partial, nch, c->cap, W.off, W.off + W.n, quad ? 1 : 0,
+  const std::vector<int> &ws = c->sys[system].wakes;
+  for (size_t k = 0; k < ws.size(); ++k) {
+    const WakeRec &W = c->wakes[ws[k]];
+    double *g = fields + k * PGPU_DIAG_FIELDS;
+    for (int m = 0; m < PGPU_DIAG_FIELDS; ++m) g[m] = 0.0;
+    const int64_t lo = std::max(W.off, row_lo), hi = std::min(W.off + W.n, row_hi);
+    if (hi <= lo) continue;
+    const int grid = (int)std::min<int64_t>(ceil_div(hi - lo, 256), c->diag_blocks);
+    diag_wake_kernel<<<grid, 256, 0, c->st>>>(c->x0, c->sig, c->partial, nch, c->cap, lo, hi, quad ? 1 : 0,
                                               c->cfg.kernel, c->d_diag);
     CK(cudaGetLastError());
     c->launches++;
     CK(cudaMemcpyAsync(h.data(), c->d_diag, (size_t)grid * kDiagFields * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    double g[kDiagFields] = {0};
+    // per-CTA partials summed in CTA order: deterministic
     for (int b = 0; b < grid; ++b)
       for (int m = 0; m < kDiagFields; ++m) g[m] += h[(size_t)b * kDiagFields + m];
-    for (int m = 0; m < kDiagFields; ++m) f[m] += g[m];
+  }
+  return PGPU_OK;
+}
+
+int pgpu_diagnose_combine(const double *fields, int32_t nwakes, double zc_prev, double *out, double *vbi,
+                          double *zc_out) {
+  if (!fields || !out || nwakes < 0) return PGPU_EINVAL;
+  double f[PGPU_DIAG_FIELDS] = {0};
+  double zc = zc_prev;
+  for (int k = 0; k < nwakes; ++k) {
+    const double *g = fields + (size_t)k * PGPU_DIAG_FIELDS;
+    for (int m = 0; m < PGPU_DIAG_FIELDS; ++m) f[m] += g[m];
+    // PAWAN's Zc: the last wake with non-zero weight wins (interaction.cpp:135-157)
     if (g[10] != 0.0) zc = g[9] / g[10];
   }
-  c->sys[system].zc = zc;
   for (int m = 0; m < 3; ++m) {
     out[m] = f[m];
     out[3 + m] = 0.5 * f[3 + m];
@@ -799,6 +919,24 @@ int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
   out[14] = zc;
   if (vbi)
     for (int m = 0; m < 3; ++m) vbi[m] = f[11 + m];
+  if (zc_out) *zc_out = zc;
+  return PGPU_OK;
+}
+
+int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
+  NvtxRange nvtx("pgpu_diagnose");
+  if (!c || !out) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (restricted(c))
+    return fail(c, PGPU_EINVAL, "with target ranges each context holds a part of the diagnostics: sum "
+                                "pgpu_diagnose_partial over the contexts and finish with pgpu_diagnose_combine");
+  if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
+  std::vector<double> fields(c->sys[system].wakes.size() * PGPU_DIAG_FIELDS);
+  int r = pgpu_diagnose_partial(c, system, fields.data());
+  if (r) return r;
+  double zc = c->sys[system].zc;
+  pgpu_diagnose_combine(fields.data(), (int32_t)c->sys[system].wakes.size(), zc, out, vbi, &zc);
+  c->sys[system].zc = zc;
   return PGPU_OK;
 }
 
@@ -928,8 +1066,9 @@ int64_t pgpu_launch_count(pgpu_ctx *c) { return c ? c->launches : -1; }
 int pgpu_pair_counts(pgpu_ctx *c, int64_t *pairs, int64_t *full_pairs) {
   if (!c) return PGPU_EINVAL;
   int64_t full = c->pairs_acc;
-  // only the FP32C Gaussian kernel has a far regime (and counts its full pairs)
-  if (c->frozen && !fp64(c) && c->cfg.kernel == PGPU_KERNEL_GAUSSIAN) {
+  // the Gaussian kernel has a far regime in both precisions (and counts its
+  // full-formula pairs); the high-order kernel evaluates every pair in full
+  if (c->frozen && c->cfg.kernel == PGPU_KERNEL_GAUSSIAN) {
     unsigned long long nf = 0;
     CK(cudaStreamSynchronize(c->st));
     CK(cudaMemcpy(&nf, c->d_nfull, sizeof(nf), cudaMemcpyDeviceToHost));
@@ -955,6 +1094,7 @@ int pgpu_autotune(pgpu_ctx *c, int reps, int *block, int *tpt, double *ms_per_la
   if (!c) return PGPU_EINVAL;
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (reps < 1) reps = 1;
+  c->sys_shape.clear();  // one shape for every system from here on
   const int saved = c->shape;
   double best = 1e300;
   int best_s = saved;
@@ -987,6 +1127,220 @@ int pgpu_autotune(pgpu_ctx *c, int reps, int *block, int *tpt, double *ms_per_la
   pgpu_pair_kernel_time(c, nullptr, nullptr);
   if (block) *block = kShapes[best_s].block;
   if (tpt) *tpt = kShapes[best_s].tpt;
+  return PGPU_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Size class of a system of n particles: class 0 holds n < 4096, class k >= 1
+// holds [1024 4^k, 1024 4^(k+1)).
+int size_class(int64_t n) {
+  int k = 0;
+  for (int64_t hi = 4096; n >= hi && k < 30; hi *= 4) ++k;
+  return k;
+}
+int64_t class_lo(int k) { return k == 0 ? 0 : (int64_t)1024 << (2 * k); }
+int64_t class_hi(int k) { return (int64_t)1024 << (2 * (k + 1)); }
+
+// Device time of one pair launch of `shape` over `systems` (their own plan and
+// chunk count), mean of `reps` launches after one untimed.
+template <typename T> int time_subset(pgpu_ctx *c, const std::vector<int> &systems, int shape, int reps, double *ms) {
+  int r = upload_plan(c);  // system sizes on the device, for the source boxes
+  if (r) return r;
+  const int nch = choose_nch_for(c, shape, systems);
+  std::vector<PlanEntry> plan = build_plan(c, systems, shape, nch);
+  plan.resize(c->sys.size() + 1, plan.back());
+  CK(cudaMemcpyAsync(c->d_plan, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  PairArgs<T> a;
+  a.P = static_cast<const v4_t<T> *>(c->P);
+  a.Q = static_cast<const v4_t<T> *>(c->Q);
+  a.partial = c->partial;
+  a.plan = c->d_plan;
+  a.nsys = (int)c->sys.size();
+  a.nch = nch;
+  a.cap = c->cap;
+  a.nu2 = (T)(2.0 * c->cfg.nu);
+  a.counters = c->d_counters;
+  a.nfull = c->d_nfull;
+  if (uses_boxes(c)) {
+    if ((r = launch_boxes(c))) return r;
+    a.box = c->d_box;
+  }
+  float total = 0.f;
+  for (int k = 0; k <= reps; ++k) {
+    CK(cudaEventRecord(c->ev[0][0], c->st));
+    pair_fn<T>(shape, c->cfg.kernel)<<<c->grid[shape], kShapes[shape].block, 0, c->st>>>(a);
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaEventRecord(c->ev[0][1], c->st));
+    CK(cudaEventSynchronize(c->ev[0][1]));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->ev[0][0], c->ev[0][1]));
+    if (k > 0) total += t;
+  }
+  *ms = total / reps;
+  return PGPU_OK;
+}
+
+std::string json_str(const std::string &line, const char *key) {
+  const std::string k = std::string("\"") + key + "\": \"";
+  const size_t p = line.find(k);
+  if (p == std::string::npos) return "";
+  const size_t e = line.find('"', p + k.size());
+  return e == std::string::npos ? "" : line.substr(p + k.size(), e - p - k.size());
+}
+
+bool json_num(const std::string &line, const char *key, double *v) {
+  const std::string k = std::string("\"") + key + "\": ";
+  const size_t p = line.find(k);
+  if (p == std::string::npos) return false;
+  char *end = nullptr;
+  *v = strtod(line.c_str() + p + k.size(), &end);
+  return end != line.c_str() + p + k.size();
+}
+
+// Times of every shape for one cached class ("ms": [..] of the line).
+bool json_ms(const std::string &line, double *ms, int n) {
+  const size_t p = line.find("\"ms\": [");
+  if (p == std::string::npos) return false;
+  const char *q = line.c_str() + p + 7;
+  for (int i = 0; i < n; ++i) {
+    char *end = nullptr;
+    ms[i] = strtod(q, &end);
+    if (end == q) return false;
+    q = end;
+    while (*q == ',' || *q == ' ') ++q;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tune_class *classes, int max_classes,
+                          int *nclasses, int *per_class) {
+  NvtxRange nvtx("pgpu_autotune_classes");
+  if (!c) return PGPU_EINVAL;
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (c->sur) return fail(c, PGPU_EINVAL, "the surrogate evaluates one system; use pgpu_autotune");
+  if (reps < 1) reps = 1;
+  int r = check_contiguous(c);
+  if (r) return r;
+  // systems by size class
+  std::map<int, std::vector<int>> cls;
+  for (size_t s = 0; s < c->sys.size(); ++s)
+    if (owned(c, (int)s).second > 0) cls[size_class(sys_n(c, (int)s))].push_back((int)s);
+  if (cls.empty()) return fail(c, PGPU_EINVAL, "no system has particles");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, c->cfg.device));
+  const std::string gpu = prop.name;
+  const std::string prec = fp64(c) ? "fp64" : "fp32c";
+  const std::string ker = c->cfg.kernel == PGPU_KERNEL_HIGHORDER ? "highorder" : "gaussian";
+  // cached times: the last matching line of the file wins
+  std::map<int, std::vector<double>> cached;
+  if (cache_path && *cache_path) {
+    if (FILE *f = fopen(cache_path, "r")) {
+      char buf[2048];
+      while (fgets(buf, sizeof(buf), f)) {
+        const std::string line(buf);
+        double k = -1;
+        std::vector<double> ms(kNumShapes);
+        if (json_str(line, "gpu") == gpu && json_str(line, "precision") == prec && json_str(line, "kernel") == ker &&
+            json_num(line, "class", &k) && json_ms(line, ms.data(), kNumShapes))
+          cached[(int)k] = ms;
+      }
+      fclose(f);
+    }
+  }
+  double ms_acc;
+  int64_t nl;
+  pgpu_pair_kernel_time(c, &ms_acc, &nl);
+  std::vector<int> keys;
+  std::vector<std::vector<double>> tms;
+  std::vector<int> from_cache;
+  for (auto &kv : cls) {
+    keys.push_back(kv.first);
+    auto it = cached.find(kv.first);
+    if (it != cached.end()) {
+      tms.push_back(it->second);
+      from_cache.push_back(1);
+      continue;
+    }
+    std::vector<double> ms(kNumShapes);
+    for (int sh = 0; sh < kNumShapes; ++sh) {
+      r = fp64(c) ? time_subset<double>(c, kv.second, sh, reps, &ms[sh]) : time_subset<float>(c, kv.second, sh, reps, &ms[sh]);
+      if (r) return r;
+    }
+    tms.push_back(ms);
+    from_cache.push_back(0);
+  }
+  // fastest shape per class, and the one shape with the least total time
+  const size_t K = keys.size();
+  std::vector<int> best(K);
+  for (size_t i = 0; i < K; ++i)
+    best[i] = (int)(std::min_element(tms[i].begin(), tms[i].end()) - tms[i].begin());
+  int single = 0;
+  double single_t = 1e300;
+  for (int sh = 0; sh < kNumShapes; ++sh) {
+    double t = 0.0;
+    for (size_t i = 0; i < K; ++i) t += tms[i][sh];
+    if (t < single_t) { single_t = t; single = sh; }
+  }
+  // one launch per class shape only if the single shape loses more than 2%
+  // on some class
+  bool split = false;
+  for (size_t i = 0; i < K; ++i)
+    if (tms[i][single] > 1.02 * tms[i][best[i]]) split = true;
+  if (split) {
+    c->sys_shape.assign(c->sys.size(), single);
+    for (size_t i = 0; i < K; ++i)
+      for (int s : cls[keys[i]]) c->sys_shape[s] = best[i];
+  } else {
+    c->sys_shape.clear();
+    c->shape = single;
+  }
+  if (cache_path && *cache_path) {
+    if (FILE *f = fopen(cache_path, "a")) {
+      for (size_t i = 0; i < K; ++i) {
+        if (from_cache[i]) continue;
+        fprintf(f, "{\"gpu\": \"%s\", \"precision\": \"%s\", \"kernel\": \"%s\", \"class\": %d, \"nmin\": %lld, "
+                   "\"nmax\": %lld, \"block\": %d, \"tpt\": %d, \"ms\": [",
+                gpu.c_str(), prec.c_str(), ker.c_str(), keys[i], (long long)class_lo(keys[i]),
+                (long long)class_hi(keys[i]), kShapes[best[i]].block, kShapes[best[i]].tpt);
+        for (int sh = 0; sh < kNumShapes; ++sh) fprintf(f, "%s%.6g", sh ? ", " : "", tms[i][sh]);
+        fprintf(f, "]}\n");
+      }
+      fclose(f);
+    } else {
+      return fail(c, PGPU_EINVAL, "cannot append to the autotune cache %s", cache_path);
+    }
+  }
+  if (nclasses) *nclasses = (int)K;
+  if (per_class) *per_class = split ? 1 : 0;
+  for (size_t i = 0; i < K && classes && (int)i < max_classes; ++i) {
+    pgpu_tune_class &o = classes[i];
+    memset(&o, 0, sizeof(o));
+    o.size_class = keys[i];
+    o.nmin = class_lo(keys[i]);
+    o.nmax = class_hi(keys[i]);
+    o.systems = (int32_t)cls[keys[i]].size();
+    o.block = kShapes[best[i]].block;
+    o.tpt = kShapes[best[i]].tpt;
+    o.from_cache = from_cache[i];
+    for (int sh = 0; sh < kNumShapes && sh < 8; ++sh) o.ms[sh] = tms[i][sh];
+    o.single_block = kShapes[single].block;
+    o.single_tpt = kShapes[single].tpt;
+  }
+  // recompute the rates of the current state with the chosen launches (the
+  // partial buffer holds the last candidate's chunks)
+  c->plan_dirty = true;
+  if ((r = upload_plan(c))) return r;
+  if ((r = pgpu_solve(c))) return r;
+  pgpu_pair_kernel_time(c, nullptr, nullptr);
   return PGPU_OK;
 }
 
@@ -1026,6 +1380,36 @@ int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops) {
     double *dst = packed ? ffma2_tflops : ffma_tflops;
     if (dst) *dst = flops / (ms * 1e-3) / 1e12;
   }
+  cudaFreeAsync(out, st);
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  return PGPU_OK;
+}
+
+int pgpu_fp64_peak(int device, double *tflops) {
+  pgpu_ctx *c = nullptr;  // for CK's error path
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float *out = nullptr;
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  CK(cudaMallocAsync((void **)&out, sizeof(float), st));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int block = 256, grid = sms * 8, iters = 1 << 12;
+  const double flops = 2.0 * kFfmaChains * (double)iters * grid * block;
+  dfma_peak_kernel<<<grid, block, 0, st>>>(out, iters, 0.999, 1e-3);  // warm-up
+  CK(cudaEventRecord(e0, st));
+  dfma_peak_kernel<<<grid, block, 0, st>>>(out, iters, 0.999, 1e-3);
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  if (tflops) *tflops = flops / (ms * 1e-3) / 1e12;
   cudaFreeAsync(out, st);
   cudaStreamSynchronize(st);
   cudaEventDestroy(e0);

@@ -30,7 +30,7 @@ constexpr int kListStack = 256;
 // 846 / 1022 / 1168 ms per evaluation with 256-particle leaves; without the
 // test, 128-particle leaves put cells within ~2 sigma in the far field and the
 // error grows to 7.5e-3.
-constexpr float kFarAccept = 16.f;
+constexpr float kFarAccept = 16.f;  // default of pgpu_surrogate_config.far_u
 
 struct TreeCell {
   int start, end;       // sorted particle range
@@ -269,7 +269,7 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
 // (kListStack); overflow sets *err, and the caller treats a non-zero *err as a
 // failed build.
 __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const int *leaves, int nleaves,
-                             float near_widths, int pass, int *far_cnt, int *near_cnt, const int *far_off,
+                             float near_widths, float far_u, int pass, int *far_cnt, int *near_cnt, const int *far_off,
                              const int *near_off, int *far_list, int2 *near_runs, int *err) {
   const int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= nleaves) return;
@@ -288,11 +288,11 @@ __global__ void lists_kernel(const TreeCell *cells, const CellData *cd, const in
     const float dx = cd[ci].v[0] - tx, dy = cd[ci].v[1] - ty, dz = cd[ci].v[2] - tz;
     const float d = sqrtf(dx * dx + dy * dy + dz * dz) - tR;
     // far: beyond near_widths cube widths, and every pair of the two cells at
-    // u = rho^2 / sigma_ij^2 >= kFarAccept, so that the Gaussian regularisation
+    // u = rho^2 / sigma_ij^2 >= far_u, so that the Gaussian regularisation
     // the singular-kernel expansion leaves out stays small
     const float gap = d - cd[ci].v[33];
     if (!contains && d >= near_widths * cd[ci].v[34] && gap > 0.f &&
-        gap * gap >= kFarAccept * (tH + cd[ci].v[39])) {
+        gap * gap >= far_u * (tH + cd[ci].v[39])) {
       if (pass) far_list[fo + nf] = ci;
       ++nf;
     } else if (c.nchild == 0) {

@@ -92,8 +92,30 @@ class GpuShard:
         """(pos, alpha) of all particles; only the owned rows are current."""
         return self.ctx.state(self.wake)
 
+    def diag_fields(self) -> np.ndarray:
+        """This rank's share of the diagnostic sums (pgpu_diagnose_partial)."""
+        return self.ctx.diagnose_partial(0)
+
     def close(self):
         self.ctx.close()
+
+
+def diagnose_dist(backend, zc_prev: float = 0.0, group=None):
+    """PAWAN's diagnose of the sharded system on every rank: each rank's
+    per-wake fields over its owned targets, summed by one all-reduce of
+    wakes x DIAG_FIELDS doubles (about 20 per wake), then combined
+    (pgpu_diagnose_combine).  Returns (record[15], vbi[3], zc)."""
+    import torch.distributed as dist
+    f = torch.as_tensor(backend.diag_fields(), dtype=torch.float64)
+    f = f.to(backend.device) if backend.device.type == "cuda" else f
+    dist.all_reduce(f, op=dist.ReduceOp.SUM, group=group)
+    return capi.diagnose_combine(f.cpu().numpy(), zc_prev)
+
+
+def diagnose_local(backends, zc_prev: float = 0.0):
+    """The same for backends of one process: the fields summed on the host."""
+    total = sum(b.diag_fields() for b in backends)
+    return capi.diagnose_combine(total, zc_prev)
 
 
 class DistExchange:

@@ -26,6 +26,10 @@ Fixtures:
                    influence(), the state after 2 RK4 and after 2 RK3 steps.
   twowake_ho.npz - twowake's inputs with the high-order kernel: rates of both
                    wakes and the diagnostics (cross-wake enstrophy terms).
+  ring5000_long.npz - the 5000-particle ring advanced by PAWAN's own __rk4
+                   (dt=0.01, nu=1e-4) for 100 steps: diagnostics at steps 0,
+                   1, 10 and 100, and the state of 256 sampled rows at steps 1,
+                   10 and 100 (about 10 minutes on 8 host cores).
 """
 from __future__ import annotations
 
@@ -125,6 +129,22 @@ def twowake_ho():
                         sha256=digest(w1) + digest(w2))
 
 
+def ring5000_long():
+    w = cases.ring_stations()
+    rows = np.sort(np.random.default_rng(321).choice(w.n, 256, replace=False))
+    R = O.RefSystem([w], NU)
+    out = {"rows": rows, "dt": 0.01, "nu": NU, "sha256": digest(w), "steps": np.array([0, 1, 10, 100])}
+    out["diag0"] = R.diagnose()
+    done = 0
+    for k in (1, 10, 100):
+        R.step("rk4", 0.01, k - done)
+        done = k
+        x, a = R.state()
+        out[f"pos{k}"], out[f"alpha{k}"] = x[rows], a[rows]
+        out[f"diag{k}"] = R.diagnose()
+    np.savez_compressed(OUT / "ring5000_long.npz", **out)
+
+
 def integrate_files():
     d = OUT / "integrate"
     d.mkdir(exist_ok=True)
@@ -134,7 +154,7 @@ def integrate_files():
 
 
 FIXTURES = {"ring1000": ring1000, "ring5000": ring5000, "twowake": twowake, "integrate": integrate_files,
-            "ring1000_ho": ring1000_ho, "twowake_ho": twowake_ho}
+            "ring1000_ho": ring1000_ho, "twowake_ho": twowake_ho, "ring5000_long": ring5000_long}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or FIXTURES:

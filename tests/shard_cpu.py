@@ -64,3 +64,10 @@ class CpuShard:
 
     def state(self):
         return self.x0[:, :3].copy(), self.x0[:, 3:].copy()
+
+    def diag_fields(self) -> np.ndarray:
+        """The owned rows' share of the diagnostic sums from the oracle's FP64
+        restatement, pair terms over every particle of the current records."""
+        rec = self.rec.numpy()
+        w = cases.Wake(rec[:, 0:3].copy(), rec[:, 3:6].copy(), self.sigma, self.vol)
+        return O.restate_diagnose_fields(w, self.first, self.first + self.count)

@@ -1,6 +1,7 @@
 """One gloo rank of the sharded-stepping test (launched twice or three times
-by tests/test_shard.py): steps a small ring with CpuShard + DistExchange and,
-on rank 0, saves the gathered state to the path in argv[1]."""
+by tests/test_shard.py): steps a small ring with CpuShard + DistExchange,
+diagnoses it with one all-reduce of the ranks' diagnostic fields and, on
+rank 0, saves the gathered state and the diagnostics to the path in argv[1]."""
 import os
 import sys
 from datetime import timedelta
@@ -25,8 +26,10 @@ def main():
     stepper = shard.ShardedStepper(b, shard.DistExchange(b))
     stepper.step("rk4", 0.01, 2)
     pos, alpha = shard.gather_state_dist(b)
+    # diagnostics of the stepped system: each rank's owned rows, one all-reduce
+    diag, vbi, zc = shard.diagnose_dist(b)
     if rank == 0:
-        np.savez(sys.argv[1], pos=pos, alpha=alpha)
+        np.savez(sys.argv[1], pos=pos, alpha=alpha, diag=diag, vbi=vbi, zc=zc)
     dist.barrier()
     dist.destroy_process_group()
 

@@ -39,7 +39,9 @@ def _free_port():
 def test_gloo_ranks_match_single_process_rk4(tmp_path, world):
     """world ranks (425 particles: ragged blocks for 2 and 3 ranks) step two
     RK4 steps, exchanging the owned source records after every stage; the
-    gathered state equals PAWAN's RK4 restated on one process."""
+    gathered state equals PAWAN's RK4 restated on one process, and the
+    diagnostics combined from the ranks' fields (pgpu_diagnose_combine after
+    an all-reduce) equal the restated diagnose of that state."""
     out = tmp_path / "state.npz"
     env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()), WORLD_SIZE=str(world),
                STATIONS="17", OMP_NUM_THREADS="1")
@@ -57,3 +59,7 @@ def test_gloo_ranks_match_single_process_rk4(tmp_path, world):
     pos, alpha = O.restate_step(w, 1e-4, "rk4", 0.01, 2)
     assert O.rel_err(got["pos"] - w.pos, pos - w.pos) < 1e-12
     assert O.rel_err(got["alpha"], alpha) < 1e-12
+    ref, vbi = O.restate_diagnose(cases.Wake(got["pos"], got["alpha"], w.sigma, w.vol))
+    scale = abs(ref[12])
+    assert np.all(np.abs(got["diag"] - ref) <= 1e-12 * np.maximum(np.abs(ref), scale))
+    assert np.all(np.abs(got["vbi"] - vbi) <= 1e-12 * np.abs(vbi).max())

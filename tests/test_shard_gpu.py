@@ -43,7 +43,7 @@ def test_target_range_rules(gpu):
         c.set_target_range(0, 100, 300)
         with pytest.raises(capi.PgpuError, match="stage by stage"):
             c.step("rk4", 0.01, 1)
-        with pytest.raises(capi.PgpuError, match="whole state"):
+        with pytest.raises(capi.PgpuError, match="pgpu_diagnose_partial"):
             c.diagnose(0)
         with pytest.raises(capi.PgpuError):
             c.surrogate_enable()
@@ -69,3 +69,59 @@ def test_records_view_the_source_records(gpu):
     assert np.allclose(P[:, 3], 0.5 * w.sigma ** 2, rtol=1e-6)
     assert np.allclose(b.Q.cpu().numpy()[:, :3], w.alpha, rtol=1e-6, atol=0)
     b.close()
+
+
+# Diagnostics of a system split over contexts: the sum of the contexts'
+# pgpu_diagnose_partial fields, combined, against pgpu_diagnose of the whole.
+# FP64: the same pair terms, summed in another order (1e-12).  FP32C: the
+# contexts' plans chunk the sources differently, which reorders FP32 group
+# sums (1e-6, far below the 1e-5 gate).
+@pytest.mark.parametrize("prec,tol", [(capi.FP64, 1e-12), (capi.FP32C, 1e-6)])
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_diagnostics_match_unsharded(gpu, prec, tol, world):
+    w = cases.ring_gaussian(stations=10, per_section=1000, seed=2)  # 10,000 particles
+    with capi.Context(precision=prec, nu=1e-4, chunks=4) as c:
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        c.step("rk4", 0.005, 2)
+        ref, ref_vbi = c.diagnose(0)
+    bs = [shard.GpuShard(w, r, world, precision=prec, nu=1e-4, chunks=4) for r in range(world)]
+    shard.ShardedStepper(bs, shard.LocalExchange(bs)).step("rk4", 0.005, 2)
+    got, vbi, zc = shard.diagnose_local(bs)
+    for b in bs:
+        b.close()
+    scale = abs(ref[12])  # kinetic energy, the scale of the quantities that vanish
+    err = np.abs(got - ref) / np.maximum(np.abs(ref), scale)
+    assert np.all(err < tol), err
+    assert np.abs(vbi - ref_vbi).max() <= tol * np.abs(ref_vbi).max()
+    assert zc == got[14]
+
+
+@pytest.mark.parametrize("prec,tol", [(capi.FP64, 1e-12), (capi.FP32C, 1e-6)])
+def test_sharded_diagnostics_two_wakes(gpu, prec, tol):
+    """Two wakes of one system (Zc from the last wake with weight, cross-wake
+    pair terms) over three target ranges that cut through both wakes."""
+    w1 = cases.ring_stations(stations=40, seed=3)
+    w2 = cases.ring_stations(R=1.2, stations=40, z0=0.3, seed=5)
+    n = w1.n + w2.n
+
+    def ctx():
+        c = capi.Context(precision=prec, nu=1e-4)
+        a, b = c.add_wake(w1.n), c.add_wake(w2.n)
+        c.set_particles(a, w1)
+        c.set_particles(b, w2)
+        return c
+
+    with ctx() as c:
+        ref, ref_vbi = c.diagnose(0)
+    parts = []
+    for r in range(3):
+        first, count, _ = shard.partition(n, 3, r)
+        with ctx() as c:
+            c.set_target_range(0, first, count)
+            parts.append(c.diagnose_partial(0))
+    assert parts[0].shape == (2, capi.DIAG_FIELDS)
+    got, vbi, zc = capi.diagnose_combine(sum(parts))
+    scale = abs(ref[12])
+    assert np.all(np.abs(got - ref) / np.maximum(np.abs(ref), scale) < tol)
+    assert np.abs(vbi - ref_vbi).max() <= tol * np.abs(ref_vbi).max()

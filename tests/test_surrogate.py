@@ -75,6 +75,18 @@ def test_gate_reverts_to_direct_sum(gpu, rings):
     assert O.rel_err(v, vd) < 2e-6 and O.rel_err(a, ad) < 2e-6
 
 
+def test_gate_also_reverts_on_dalpha_error(gpu, rings):
+    """A tolerance between the sampled velocity error and the larger sampled
+    dalpha/dt error: the velocity alone would pass, the stretching does not."""
+    _, _, st = surrogate(rings, order=1, tolerance=1.0)
+    ev, ea = st["last_err_vel"], st["last_err_dalpha"]
+    assert ea > ev > 0
+    vd, ad = direct(rings)
+    v, a, st = surrogate(rings, order=1, tolerance=0.5 * (ev + ea))
+    assert st["fallbacks"] == 1 and st["max_err_dalpha"] == st["last_err_dalpha"]
+    assert O.rel_err(v, vd) < 2e-6 and O.rel_err(a, ad) < 2e-6
+
+
 def test_surrogate_rk4_steps_track_direct(gpu):
     w = cases.leapfrog_rings(n_total=100_000)
     out = []
@@ -129,3 +141,24 @@ def test_octree_partitions_particles(gpu):
     order = np.argsort(lv[:, 0])
     assert lv[order[0], 0] == 0 and lv[order[-1], 1] == w.n and np.all(lv[order][1:, 0] == lv[order][:-1, 1])
     assert np.all(lv[:, 1] - lv[:, 0] <= 64)
+
+
+@pytest.mark.parametrize("case", ["ring1m", "leapfrog1m"])
+def test_surrogate_vs_fp64_restatement(gpu, case):
+    """The quadrupole far field at 1M particles (the configuration-2 ring, and
+    two coaxial leapfrogging rings) against the oracle's FP64 restatement of
+    PAWAN's pair sum on 256 seeded targets: velocity and dalpha/dt both within
+    the 1e-4 gate, with no fallback (so the surrogate's own result is what is
+    compared)."""
+    if case == "ring1m":
+        w = cases.ring_gaussian(stations=1000, per_section=1000, sigma=0.02, seed=1)
+    else:
+        w = cases.leapfrog_rings(n_total=1_000_000)
+    v, a, st = surrogate(w, order=2, tolerance=1e-4, check_targets=4096)
+    assert st["fallbacks"] == 0, st
+    rows = np.sort(np.random.default_rng(5).choice(w.n, 256, replace=False))
+    vr, ar = O.restate_rates(w, 1e-4, targets=rows)
+    ev, ea = O.rel_err(v[rows], vr), O.rel_err(a[rows], ar)
+    print(f"{case}: surrogate vs FP64 restatement, velocity {ev:.2e}, dalpha/dt {ea:.2e}; sampled gate "
+          f"{st['last_err_vel']:.2e} / {st['last_err_dalpha']:.2e}")
+    assert ev <= 1e-4 and ea <= 1e-4
