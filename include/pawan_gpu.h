@@ -62,6 +62,12 @@ typedef struct pgpu_config {
                       diagnostics (enstrophy and enstrophyF are non-zero only for the
                       high-order kernel, as in PAWAN), probes and the vorticity field all
                       use it.  The far-field surrogate supports the Gaussian kernel only. */
+  int split_positions; /* FP32C with the Gaussian kernel: keep each position as its FP32 value plus the
+                          FP32 residual of the FP64 state, and form the differences of nearby pairs
+                          (tiles with a pair at rho^2 < 50 sigma^2) from both, so that dense filaments,
+                          whose pair distances are a few hundred FP32 ulps of the coordinates, keep
+                          FP64-quality differences.  Costs 16 B per particle and a few operations per
+                          near pair; not supported with target ranges.  Default 0. */
 } pgpu_config;
 
 /* Fills cfg with defaults (FP32C, device 0, nu = 1.56e-5 as __interaction(),
@@ -298,9 +304,9 @@ int pgpu_autotune_classes(pgpu_ctx *ctx, int reps, const char *cache_path, pgpu_
  * surrogate never returns an unchecked result when check_targets > 0). */
 typedef struct pgpu_surrogate_config {
   int leaf_size;       /* particles per octree leaf, 1..512 (default 256) */
-  double near_widths;  /* near field: cells closer than this many cube widths (default 4) */
+  double near_widths;  /* near field: cells closer than this many cube widths (default 5) */
   int order;           /* far-field expansion: 0 monopole, 1 + dipole, 2 + quadrupole (default) */
-  int use_mlp;         /* add the learned correction to the order-1 far field (pgpu_surrogate_set_mlp) */
+  int use_mlp;         /* add the learned correction to the far field of `order` (pgpu_surrogate_set_mlp) */
   double tolerance;    /* maximum relative error of the velocity and of dalpha/dt on the sampled targets
                           (default 1e-4) */
   int check_targets;   /* targets re-checked by the direct sum per evaluation (default 4096, 0 = off) */
@@ -339,10 +345,13 @@ int pgpu_surrogate_tree(pgpu_ctx *ctx, int *idx, int64_t idx_cap, int *cell, int
 /* ---------------------------------------------------------------------------
  * Far-field correction network (no PAWAN counterpart).  A 24-128-128-128-6
  * GELU MLP whose products run on the tensor cores in BF16 with FP32
- * accumulation (forward, backward and Adam are this library's kernels).  It
- * predicts, per (target, far cell) pair, the residual of the monopole+dipole
- * expansion from the cell's moments and the target offset; the features and
- * output scales are documented in pawan_b200/csrc/treeeval.cuh.  Parameters
+ * accumulation (forward, backward and Adam are this library's kernels:
+ * training and pgpu_mlp_forward on the tcgen05 tensor cores with TMEM
+ * accumulators, the far field's fused per-warp path on mma.sync).  It
+ * predicts, per (target, far cell) pair, the residual of the multipole
+ * expansion of the order it was trained against, from the cell's moments and
+ * the target offset; the features and output scales are documented in
+ * pawan_b200/csrc/treeeval.cuh.  Parameters
  * are pgpu_mlp_num_params() floats: W1[32][128] (rows 24..31 zero), b1[128],
  * W2[128][128], b2[128], W3[128][128], b3[128], W4[128][8] (columns 6, 7
  * zero), b4[8]; a row times W is the layer's pre-activation. */
@@ -362,7 +371,8 @@ int pgpu_mlp_forward_fused(pgpu_mlp *mlp, const float *x, int64_t rows, float *y
 int pgpu_mlp_gradient(pgpu_mlp *mlp, const float *x, const float *t, int64_t rows, float *grad, double *loss);
 /* Training set: replace with host rows, or append rows drawn from the octree
  * of a context's last surrogate evaluation (targets are the exact direct-sum
- * contribution of the cell minus its monopole+dipole expansion, scaled). */
+ * contribution of the cell minus its expansion to the context's surrogate
+ * order, scaled). */
 int pgpu_mlp_set_dataset(pgpu_mlp *mlp, const float *x, const float *t, int64_t rows);
 int pgpu_mlp_add_samples(pgpu_mlp *mlp, pgpu_ctx *ctx, int64_t nsamples, int seed);
 int64_t pgpu_mlp_dataset_rows(pgpu_mlp *mlp);
@@ -370,7 +380,8 @@ int pgpu_mlp_get_dataset(pgpu_mlp *mlp, float *x, float *t, int64_t max_rows);
 /* Adam (beta 0.9 / 0.999) on random minibatches; loss_history[steps] may be NULL. */
 int pgpu_mlp_train(pgpu_mlp *mlp, int steps, int batch, double lr, int seed, float *loss_history);
 /* Uses a snapshot of the network's current weights for the surrogate's far
- * field (order-1 expansion + correction) when use_mlp is set. */
+ * field (expansion to the configured order + correction) when use_mlp is set;
+ * the network should have been trained on samples drawn at that order. */
 int pgpu_surrogate_set_mlp(pgpu_ctx *ctx, pgpu_mlp *mlp);
 
 /* The context's CUDA stream (a cudaStream_t), so a caller can order its own

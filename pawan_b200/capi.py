@@ -50,7 +50,7 @@ EXPORTS = [
 class PgpuConfig(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("nu", C.c_double), ("vinf", C.c_double * 3),
                 ("block", C.c_int), ("tpt", C.c_int), ("chunks", C.c_int), ("use_graphs", C.c_int),
-                ("kernel", C.c_int)]
+                ("kernel", C.c_int), ("split_positions", C.c_int)]
 
 
 class SurrogateConfig(C.Structure):
@@ -258,7 +258,8 @@ class Context:
     """One backend context: wakes grouped into systems, all device-resident."""
 
     def __init__(self, precision: int = FP32C, nu: float = 1.56e-5, device: int = 0, vinf=(0.0, 0.0, 0.0),
-                 block: int = 0, tpt: int = 0, chunks: int = 0, use_graphs: bool = True, kernel: int = GAUSSIAN):
+                 block: int = 0, tpt: int = 0, chunks: int = 0, use_graphs: bool = True, kernel: int = GAUSSIAN,
+                 split_positions: bool = False):
         self.lib = load()
         cfg = PgpuConfig()
         self.lib.pgpu_config_default(C.byref(cfg))
@@ -270,6 +271,7 @@ class Context:
         cfg.block, cfg.tpt, cfg.chunks = block, tpt, chunks
         cfg.use_graphs = 1 if use_graphs else 0
         cfg.kernel = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+        cfg.split_positions = 1 if split_positions else 0
         h = C.c_void_p()
         rc = self.lib.pgpu_create(C.byref(h), C.byref(cfg))
         if rc != PGPU_OK:

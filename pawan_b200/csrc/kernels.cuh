@@ -33,7 +33,7 @@ namespace pgpu {
 constexpr int kMaxChunks = 16;
 // Sources per compensation group of the FP32 pair kernel: plain FP32 partial
 // sums over this many sources, then one error-free two-sum per component.
-constexpr int kPairCG = 64;
+constexpr int kPairCG = 128;
 constexpr int kDiagFields = 23;
 // FP64 far regime: u = rho^2 / sigma^2 >= 100, where erfc(sqrt(u/2)) and the
 // e^{-u/2} terms of q and F vanish at double precision (the closed form and
@@ -69,6 +69,10 @@ template <typename T> struct PairArgs {
   // source tile is a run of whole blocks.  nullptr: the FP32 kernel reduces
   // each tile's box itself.
   const float4 *box = nullptr;
+  // Split positions (FP32C, pgpu_config.split_positions): the FP32 rounding
+  // residuals (x - (float)x, y - (float)y, z - (float)z, 0) of every
+  // particle, added to the pair differences in tiles with near pairs.
+  const float4 *L = nullptr;
 };
 
 // Slots per precomputed source box (divides every pair-kernel tile).
@@ -507,15 +511,23 @@ constexpr int pair_min_blocks() {
                                                             : 1;
 }
 
-template <typename T, int BLOCK, int TPT, int CG, int KER = kGaussian>
+// SPLIT: the FP32 Gaussian body with split positions (PairArgs::L).
+template <typename T, int BLOCK, int TPT, int CG, int KER = kGaussian, bool SPLIT = false>
 __global__ void __launch_bounds__(BLOCK, (pair_min_blocks<T, BLOCK, TPT, KER>())) pair_kernel(PairArgs<T> a) {
   constexpr int kCG = CG < BLOCK ? CG : BLOCK;  // a group never spans more than one tile
-  if constexpr (sizeof(T) == 4 && KER == kGaussian) pair_body_f32<BLOCK, TPT, kCG>(a);
+  if constexpr (sizeof(T) == 4 && KER == kGaussian) pair_body_f32<BLOCK, TPT, kCG, SPLIT>(a);
   else pair_body_generic<T, BLOCK, TPT, kCG, KER>(a);
 }
 
 // ---------------------------------------------------------------- stage kernel
+// FP32 residuals of a position after rounding to FP32: x - (float)x exactly
+// (Sterbenz), then rounded to FP32, so (float)x + residual carries ~48 bits.
+__device__ __forceinline__ float4 split_low(double x, double y, double z) {
+  return make_float4((float)(x - (double)(float)x), (float)(y - (double)(float)y), (float)(z - (double)(float)z), 0.f);
+}
+
 struct StageArgs {
+  float4 *L = nullptr;  // split-position residuals, rewritten with the records (FP32C, split positions)
   double *x0;          // [6][cap] FP64 state (x, y, z, ax, ay, az) at the step start
   double *acc;         // [6][cap] RK accumulator
   double *rates;       // [6][cap] last evaluated rates (velocity, dalpha)
@@ -629,18 +641,21 @@ __global__ void stage_kernel(StageArgs a) {
     const double sg = a.sig[i];
     static_cast<v4_t<T> *>(a.P)[i] = make_v4<T>((T)y[0], (T)y[1], (T)y[2], (T)(0.5 * sg * sg));
     static_cast<v4_t<T> *>(a.Q)[i] = make_v4<T>((T)y[3], (T)y[4], (T)y[5], (T)a.vol[i]);
+    if (a.L) a.L[i] = split_low(y[0], y[1], y[2]);
   }
 }
 
-// Pack the FP64 state at the step start into the source records.
+// Pack the FP64 state at the step start into the source records (and the
+// split-position residuals when L is set).
 template <typename T>
-__global__ void pack_kernel(const double *x0, const double *sig, const double *vol, void *P, void *Q, int64_t lo,
-                            int64_t hi, int64_t cap) {
+__global__ void pack_kernel(const double *x0, const double *sig, const double *vol, void *P, void *Q, float4 *L,
+                            int64_t lo, int64_t hi, int64_t cap) {
   for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
     const double sg = sig[i];
     static_cast<v4_t<T> *>(P)[i] = make_v4<T>((T)x0[i], (T)x0[cap + i], (T)x0[2 * cap + i], (T)(0.5 * sg * sg));
     static_cast<v4_t<T> *>(Q)[i] =
         make_v4<T>((T)x0[3 * cap + i], (T)x0[4 * cap + i], (T)x0[5 * cap + i], (T)vol[i]);
+    if (L) L[i] = split_low(x0[i], x0[cap + i], x0[2 * cap + i]);
   }
 }
 

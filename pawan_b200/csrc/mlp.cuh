@@ -1,10 +1,11 @@
 // Far-field correction network: 24 -> 128 -> 128 -> 128 -> 6, GELU (tanh
 // form, Hendrycks & Gimpel 2016), BF16 tensor-core products with FP32
-// accumulation (mma.sync.m16n8k16), FP32 master weights, Adam.
+// accumulation, FP32 master weights, Adam.
 //
-// Training uses one generic tiled GEMM (C = op(A) op(B), 64x64x32 CTA tiles,
-// four warps of 32x32) with fused epilogues (bias + GELU forward, GELU'
-// backward, split-K accumulation for weight gradients).  Inference inside the
+// Training and the batch forward use one generic GEMM on the tcgen05 tensor
+// cores (C = op(A) op(B), 128-row CTA tiles, accumulator in TMEM;
+// mlp_tc.cuh) with fused epilogues (bias + GELU forward, GELU' backward,
+// split-K accumulation for weight gradients).  Inference inside the
 // far-field evaluation runs the whole network per warp on 16-row tiles with
 // activations kept in registers: the FP32 accumulator fragment of one layer is
 // the BF16 A fragment of the next (same thread-to-element map), so hidden
@@ -70,85 +71,6 @@ struct GemmArgs {
   int ksplit;  // K range per blockIdx.z
 };
 
-constexpr int kGBM = 64, kGBN = 64, kGBK = 32;
-
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
-  __shared__ __align__(16) __nv_bfloat16 As[kGBM][kGBK + 8];
-  __shared__ __align__(16) __nv_bfloat16 Bs[kGBN][kGBK + 8];  // stored transposed: Bs[n][k]
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.y * kGBM, n0 = blockIdx.x * kGBN;
-  const int kz0 = blockIdx.z * g.ksplit, kz1 = min(g.K, kz0 + g.ksplit);
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int gid = lane >> 2, tig = lane & 3;
-  float acc[2][4][4];
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 4; ++j)
-      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
-  for (int k0 = kz0; k0 < kz1; k0 += kGBK) {
-    __syncthreads();
-    for (int e = tid; e < kGBM * kGBK; e += 128) {
-      const int r = e / kGBK, c = e % kGBK;
-      const int m = m0 + r, k = k0 + c;
-      float v = 0.f;
-      if (m < g.M && k < kz1) v = g.transA ? g.A[(int64_t)k * g.lda + m] : g.A[(int64_t)m * g.lda + k];
-      As[r][c] = __float2bfloat16_rn(v);
-    }
-    for (int e = tid; e < kGBN * kGBK; e += 128) {
-      const int r = e / kGBK, c = e % kGBK;  // r = n, c = k
-      const int n = n0 + r, k = k0 + c;
-      float v = 0.f;
-      if (n < g.N && k < kz1) v = g.transB ? g.B[(int64_t)n * g.ldb + k] : g.B[(int64_t)k * g.ldb + n];
-      Bs[r][c] = __float2bfloat16_rn(v);
-    }
-    __syncthreads();
-    for (int ks = 0; ks < kGBK; ks += 16) {
-      uint32_t a[2][4], b[4][2];
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm + i * 16 + gid, c = ks + tig * 2;
-        a[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][c]);
-        a[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][c]);
-        a[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][c + 8]);
-        a[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][c + 8]);
-      }
-      for (int j = 0; j < 4; ++j) {
-        const int n = wn + j * 8 + gid, c = ks + tig * 2;
-        b[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[n][c]);
-        b[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[n][c + 8]);
-      }
-      for (int i = 0; i < 2; ++i)
-        for (int j = 0; j < 4; ++j) mma_16816(acc[i][j], a[i], b[j]);
-    }
-  }
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 4; ++j)
-      for (int e = 0; e < 4; ++e) {
-        const int m = m0 + wm + i * 16 + gid + (e >> 1) * 8;
-        const int n = n0 + wn + j * 8 + tig * 2 + (e & 1);
-        if (m >= g.M || n >= g.N) continue;
-        const int64_t o = (int64_t)m * g.ldc + n;
-        float v = acc[i][j][e];
-        switch (g.epi) {
-          case kEpiBiasGelu:
-            v += g.bias[n];
-            g.C[o] = v;
-            g.H[o] = gelu_f(v);
-            break;
-          case kEpiBias:
-            g.C[o] = v + g.bias[n];
-            break;
-          case kEpiGeluGrad:
-            g.C[o] = v * gelu_grad(g.Z[o]);
-            break;
-          case kEpiAtomic:
-            atomicAdd(&g.C[o], v);
-            break;
-          default:
-            g.C[o] = v;
-        }
-      }
-}
-
-// Column sums (bias gradients): out[n] += sum_m X[m*ld + n].
 __global__ void colsum_kernel(const float *X, int M, int N, int ld, float *out) {
   const int n = blockIdx.x;
   float s = 0.f;
@@ -343,3 +265,5 @@ __global__ void gather_batch_kernel(const float *Xd, const float *Td, const int 
 }
 
 }  // namespace pgpu
+
+#include "mlp_tc.cuh"

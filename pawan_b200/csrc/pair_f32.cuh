@@ -42,7 +42,7 @@ constexpr int pair_f32_min_blocks() {
 // of each other on B200; 2 is best with the autotuner's usual 128x2 shape).
 constexpr int kF32Unroll = 2;
 
-template <int BLOCK, int TPT, int CG>
+template <int BLOCK, int TPT, int CG, bool SPLIT>
 __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
   constexpr int TILE = BLOCK;
   constexpr int TT = BLOCK * TPT;
@@ -50,6 +50,9 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
   static_assert(TILE % CG == 0 && CG % 2 == 0, "compensation group must divide the tile into source pairs");
   __shared__ __align__(16) float4 sP[2][TILE];
   __shared__ __align__(16) float4 sQ[2][TILE];
+  // split positions: the sources' FP32 residuals, pair-interleaved like sP
+  // (float4 2r = (xl0, xl1, yl0, yl1), 2r+1 = (zl0, zl1, -, -))
+  __shared__ __align__(16) float4 sL[SPLIT ? 2 : 1][SPLIT ? TILE : 1];
   __shared__ __align__(16) float4 sN[TILE];  // n_s = (x_s - ref) x alpha_s, pair-interleaved like sP
   __shared__ int s_item;
   const int tid = threadIdx.x;
@@ -71,6 +74,7 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
     // targets: positions duplicated into both float2 lanes (lane .x serves
     // the scalar code); scalar strength, sigma^2/2 and volume
     float at[TPT][3], hst[TPT], vt[TPT], h50[TPT];
+    float xl[SPLIT ? TPT : 1][3];  // targets' position residuals (split positions)
     float2 X[TPT][3], AT3[TPT][3];
     float vh[TPT][3], vl[TPT][3], dh[TPT][3], dl[TPT][3];
     unsigned nfull = 0;  // pairs evaluated with the full (non-far) formula, self pairs included
@@ -80,6 +84,10 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
       ti = ti < tend ? ti : tend - 1;
       const float4 p = a.P[ti];
       const float4 q = a.Q[ti];
+      if constexpr (SPLIT) {
+        const float4 l = a.L[ti];
+        xl[k][0] = l.x; xl[k][1] = l.y; xl[k][2] = l.z;
+      }
       hst[k] = p.w;
       h50[k] = kFarU * p.w;
       at[k][0] = q.x; at[k][1] = q.y; at[k][2] = q.z; vt[k] = q.w;
@@ -112,6 +120,16 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
         // padding source: far away, zero strength and volume (pad_P / pad_Q)
         dp[0] = 1e18f; dp[2] = 1e18f; dp[4] = 1e18f; dp[6] = 1.f;
         dq[0] = 0.f; dq[2] = 0.f; dq[4] = 0.f; dq[6] = 0.f;
+      }
+      if constexpr (SPLIT) {
+        float *dl = reinterpret_cast<float *>(&sL[b][0]) + (tid >> 1) * 8 + (tid & 1);
+        if (j < s1) {
+          const float *gl = reinterpret_cast<const float *>(a.L + j);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) cp_async4(dl + 2 * m, gl + m);
+        } else {
+          dl[0] = 0.f; dl[2] = 0.f; dl[4] = 0.f;
+        }
       }
     };
 
@@ -166,10 +184,12 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
           sbox.hi[2] = fmaxf(sbox.hi[2], hi.z);
         }
       } else {
+        // the tile's real sources only (not the padding), as the precomputed boxes
+        const int nvalid = (int)min((int64_t)TILE, s1 - sb);
         for (int r = lane; r < NPR; r += 32) {
           const float4 u = sP[buf][2 * r], v = sP[buf][2 * r + 1];
-          sbox.add(u.x, u.z, v.x, v.z);
-          sbox.add(u.y, u.w, v.y, v.w);
+          if (2 * r < nvalid) sbox.add(u.x, u.z, v.x, v.z);
+          if (2 * r + 1 < nvalid) sbox.add(u.y, u.w, v.y, v.w);
         }
         sbox.reduce();
       }
@@ -245,10 +265,16 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
         } else {
           // Tiles with possible near pairs: scalar, one source at a time,
           // accumulated into lane .x.
-          auto one = [&](float sx, float sy, float sz, float shs, float qx, float qy, float qz, float qv) {
+          auto one = [&](float sx, float sy, float sz, float shs, float qx, float qy, float qz, float qv, float lx,
+                         float ly, float lz) {
 #pragma unroll
             for (int k = 0; k < TPT; ++k) {
-              const float dx = X[k][0].x - sx, dy = X[k][1].x - sy, dz = X[k][2].x - sz;
+              float dx = X[k][0].x - sx, dy = X[k][1].x - sy, dz = X[k][2].x - sz;
+              if constexpr (SPLIT) {
+                // the FP32 difference of nearby positions is exact; adding the
+                // difference of the residuals restores the FP64 difference
+                dx += xl[k][0] - lx; dy += xl[k][1] - ly; dz += xl[k][2] - lz;
+              }
               const float r2 = dx * dx + dy * dy + dz * dz;
               // far test r^2 >= 50 (hs_t + hs_s) as one FMA against the
               // target's precomputed 50 hs_t
@@ -290,8 +316,10 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
           for (int r = g; r < g + CG / 2; ++r) {
             const float4 pa = sP[buf][2 * r], pb = sP[buf][2 * r + 1];
             const float4 qa = sQ[buf][2 * r], qb = sQ[buf][2 * r + 1];
-            one(pa.x, pa.z, pb.x, pb.z, qa.x, qa.z, qb.x, qb.z);
-            one(pa.y, pa.w, pb.y, pb.w, qa.y, qa.w, qb.y, qb.w);
+            float4 la = make_float4(0.f, 0.f, 0.f, 0.f), lb = la;
+            if constexpr (SPLIT) { la = sL[buf][2 * r]; lb = sL[buf][2 * r + 1]; }
+            one(pa.x, pa.z, pb.x, pb.z, qa.x, qa.z, qb.x, qb.z, la.x, la.z, lb.x);
+            one(pa.y, pa.w, pb.y, pb.w, qa.y, qa.w, qb.y, qb.w, la.y, la.w, lb.y);
           }
         }
 #pragma unroll

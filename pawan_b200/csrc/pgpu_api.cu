@@ -47,19 +47,24 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 template <typename T> using PairFn = void (*)(PairArgs<T>);
 
-template <typename T, int KER> PairFn<T> pair_fn_k(int s) {
+template <typename T, int KER, bool SPLIT = false> PairFn<T> pair_fn_k(int s) {
   switch (s) {
-    case 0: return pair_kernel<T, 128, 1, kCG, KER>;
-    case 1: return pair_kernel<T, 128, 2, kCG, KER>;
-    case 2: return pair_kernel<T, 256, 1, kCG, KER>;
-    case 3: return pair_kernel<T, 256, 2, kCG, KER>;
-    case 4: return pair_kernel<T, 64, 2, kCG, KER>;
-    default: return pair_kernel<T, 128, 4, kCG, KER>;
+    case 0: return pair_kernel<T, 128, 1, kCG, KER, SPLIT>;
+    case 1: return pair_kernel<T, 128, 2, kCG, KER, SPLIT>;
+    case 2: return pair_kernel<T, 256, 1, kCG, KER, SPLIT>;
+    case 3: return pair_kernel<T, 256, 2, kCG, KER, SPLIT>;
+    case 4: return pair_kernel<T, 64, 2, kCG, KER, SPLIT>;
+    default: return pair_kernel<T, 128, 4, kCG, KER, SPLIT>;
   }
 }
-// Pair kernel of shape s for regularisation kernel `ker` (PGPU_KERNEL_*).
-template <typename T> PairFn<T> pair_fn(int s, int ker) {
-  return ker == PGPU_KERNEL_HIGHORDER ? pair_fn_k<T, kHighOrder>(s) : pair_fn_k<T, kGaussian>(s);
+// Pair kernel of shape s for regularisation kernel `ker` (PGPU_KERNEL_*);
+// split: the FP32C Gaussian body with split positions.
+template <typename T> PairFn<T> pair_fn(int s, int ker, bool split) {
+  if (ker == PGPU_KERNEL_HIGHORDER) return pair_fn_k<T, kHighOrder>(s);
+  if constexpr (sizeof(T) == 4) {
+    if (split) return pair_fn_k<T, kGaussian, true>(s);
+  }
+  return pair_fn_k<T, kGaussian>(s);
 }
 
 struct WakeRec {
@@ -98,6 +103,7 @@ struct pgpu_ctx {
   unsigned int *d_counters = nullptr;
   unsigned long long *d_nfull = nullptr;
   float4 *d_box = nullptr;  // FP32 source boxes per kBoxGran slots (box_kernel), FP32C Gaussian contexts
+  float4 *d_L = nullptr;    // [cap] split-position residuals (pgpu_config.split_positions)
   int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
   int *d_flag = nullptr;
   int diag_blocks = 0;
@@ -158,6 +164,8 @@ bool fp64(const pgpu_ctx *c) { return c->cfg.precision == PGPU_FP64; }
 // The FP32C Gaussian pair kernel tests whole source tiles against boxes
 // precomputed per kBoxGran slots (box_kernel) before each launch.
 bool uses_boxes(const pgpu_ctx *c) { return !fp64(c) && c->cfg.kernel == PGPU_KERNEL_GAUSSIAN; }
+// Split positions: FP32C Gaussian contexts with pgpu_config.split_positions.
+bool uses_split(const pgpu_ctx *c) { return uses_boxes(c) && c->cfg.split_positions != 0; }
 // Boxes cover every slot plus one largest tile (256 slots) past the last:
 // the last tile of the last system may end beyond `cap`, and those blocks
 // hold empty boxes.
@@ -187,7 +195,7 @@ int check_contiguous(pgpu_ctx *c) {
 
 template <typename T> int occupancy(pgpu_ctx *c, int s) {
   int nb = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pair_fn<T>(s, c->cfg.kernel), kShapes[s].block, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pair_fn<T>(s, c->cfg.kernel, uses_split(c)), kShapes[s].block, 0);
   if (e != cudaSuccess || nb < 1) nb = 1;
   return nb * c->sms;
 }
@@ -238,6 +246,10 @@ int freeze(pgpu_ctx *c) {
   if ((r = alloc((void **)&c->d_counters, 4 * sizeof(unsigned int)))) return r;
   if ((r = alloc((void **)&c->d_nfull, sizeof(unsigned long long)))) return r;
   if (uses_boxes(c) && (r = alloc((void **)&c->d_box, 2 * box_blocks(c) * sizeof(float4)))) return r;
+  if (uses_split(c)) {
+    if ((r = alloc((void **)&c->d_L, cap * sizeof(float4)))) return r;
+    CK(cudaMemsetAsync(c->d_L, 0, cap * sizeof(float4), c->st));
+  }
   if ((r = alloc((void **)&c->d_flag, sizeof(int)))) return r;
   c->diag_blocks = 2 * c->sms;
   if ((r = alloc((void **)&c->d_diag, (size_t)c->diag_blocks * kDiagFields * sizeof(double)))) return r;
@@ -443,12 +455,13 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
     if (r) return r;
     a.box = c->d_box;
   }
+  a.L = c->d_L;
   // Inside stream capture an event record only becomes a timestamp node of
   // the graph when it is marked external.
   const unsigned flags = c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (c->timing && slot >= 0) CK(cudaEventRecordWithFlags(c->ev[slot][0], c->st, flags));
   if (c->groups.empty()) {
-    pair_fn<T>(c->shape, c->cfg.kernel)<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
+    pair_fn<T>(c->shape, c->cfg.kernel, uses_split(c))<<<c->grid[c->shape], kShapes[c->shape].block, 0, c->st>>>(a);
     CK(cudaGetLastError());
     c->launches++;
   } else {
@@ -457,7 +470,7 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
     for (size_t g = 0; g < c->groups.size(); ++g) {
       const int sh = c->groups[g];
       a.plan = c->d_plan + g * (c->sys.size() + 1);
-      pair_fn<T>(sh, c->cfg.kernel)<<<c->grid[sh], kShapes[sh].block, 0, c->st>>>(a);
+      pair_fn<T>(sh, c->cfg.kernel, uses_split(c))<<<c->grid[sh], kShapes[sh].block, 0, c->st>>>(a);
       CK(cudaGetLastError());
       c->launches++;
     }
@@ -469,7 +482,7 @@ template <typename T> int launch_pair(pgpu_ctx *c, int slot) {
 
 int launch_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
   StageArgs s;
-  s.x0 = c->x0; s.acc = c->acc; s.rates = c->rates; s.sig = c->sig; s.vol = c->vol;
+  s.x0 = c->x0; s.acc = c->acc; s.rates = c->rates; s.sig = c->sig; s.vol = c->vol; s.L = c->d_L;
   s.partial = c->partial; s.P = c->P; s.Q = c->Q;
   s.sys_off = c->d_sysoff; s.sys_n = c->d_sysn; s.sys_t = c->d_syst; s.nsys = (int)c->sys.size();
   s.nch = c->nch; s.cap = c->cap; s.scheme = scheme; s.stage = stage; s.dt = dt;
@@ -488,8 +501,8 @@ int launch_pack(pgpu_ctx *c, int64_t lo, int64_t hi) {
   if (hi <= lo) return PGPU_OK;
   const int block = 256;
   const int grid = (int)std::min<int64_t>(ceil_div(hi - lo, block), 16LL * c->sms);
-  if (fp64(c)) pack_kernel<double><<<grid, block, 0, c->st>>>(c->x0, c->sig, c->vol, c->P, c->Q, lo, hi, c->cap);
-  else pack_kernel<float><<<grid, block, 0, c->st>>>(c->x0, c->sig, c->vol, c->P, c->Q, lo, hi, c->cap);
+  if (fp64(c)) pack_kernel<double><<<grid, block, 0, c->st>>>(c->x0, c->sig, c->vol, c->P, c->Q, nullptr, lo, hi, c->cap);
+  else pack_kernel<float><<<grid, block, 0, c->st>>>(c->x0, c->sig, c->vol, c->P, c->Q, c->d_L, lo, hi, c->cap);
   CK(cudaGetLastError());
   c->launches++;
   return PGPU_OK;
@@ -613,7 +626,7 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (auto g : c->graph_defs) cudaGraphDestroy(g);
   void *ptrs[] = {c->x0, c->acc, c->rates, c->sig, c->vol, c->partial, c->stage, c->d_diag, c->P, c->Q,
                   c->d_sysoff, c->d_sysn, c->d_syst, c->d_plan, c->d_plan_diag, c->d_plan_field, c->d_field,
-                  c->d_counters, c->d_nfull, c->d_flag, c->d_merge, c->d_merge_tmp, c->d_box};
+                  c->d_counters, c->d_nfull, c->d_flag, c->d_merge, c->d_merge_tmp, c->d_box, c->d_L};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
@@ -757,6 +770,8 @@ int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t co
   if (!c) return PGPU_EINVAL;
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   if (c->sur) return fail(c, PGPU_EINVAL, "the surrogate evaluates every target of its system");
+  if (uses_split(c) && count >= 0)
+    return fail(c, PGPU_EINVAL, "split positions are not exchanged between contexts: use one context per system");
   if (count >= 0 && first < 0) return fail(c, PGPU_EINVAL, "negative first target %lld", (long long)first);
   SysRec &S = c->sys[system];
   S.t_first = count < 0 ? 0 : first;
@@ -1169,10 +1184,11 @@ template <typename T> int time_subset(pgpu_ctx *c, const std::vector<int> &syste
     if ((r = launch_boxes(c))) return r;
     a.box = c->d_box;
   }
+  a.L = c->d_L;
   float total = 0.f;
   for (int k = 0; k <= reps; ++k) {
     CK(cudaEventRecord(c->ev[0][0], c->st));
-    pair_fn<T>(shape, c->cfg.kernel)<<<c->grid[shape], kShapes[shape].block, 0, c->st>>>(a);
+    pair_fn<T>(shape, c->cfg.kernel, uses_split(c))<<<c->grid[shape], kShapes[shape].block, 0, c->st>>>(a);
     CK(cudaGetLastError());
     c->launches++;
     CK(cudaEventRecord(c->ev[0][1], c->st));

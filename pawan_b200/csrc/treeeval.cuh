@@ -432,8 +432,9 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
 // Training samples of the correction network from the current octree: each
 // warp draws (leaf, target, far cell) with a hash of (seed, sample), computes
 // the features, the exact FP64 contribution of the cell's particles (the
-// direct kernel's formula) and the order-1 expansion, and stores the scaled
-// residual.  Rows whose leaf has no far cell after 32 draws are all zero.
+// direct kernel's formula) and the expansion to the surrogate's order
+// (a.order), and stores the scaled residual.  Rows whose leaf has no far cell
+// after 32 draws are all zero.
 __global__ void mlp_sample_kernel(TreeEvalArgs a, const int *far_leaves, int nfar_leaves, int nsamples,
                                   unsigned long long seed, float *X, float *T) {
   const int lane = threadIdx.x & 31;
@@ -484,7 +485,7 @@ __global__ void mlp_sample_kernel(TreeEvalArgs a, const int *far_leaves, int nfa
     if (lane == 0) {
       float f[kIn], scv, scs, u[3], s[3];
       far_features(v, xt, at, f, scv, scs);
-      far_expand(v, xt, at, 1, u, s);
+      far_expand(v, xt, at, a.order, u, s);
       for (int i = 0; i < kIn; ++i) xo[i] = f[i];
       for (int m = 0; m < 3; ++m) {
         to[m] = scv > 0.f ? (float)((ex[m] - u[m]) / scv) : 0.f;

@@ -82,13 +82,17 @@ def test_training_reduces_loss(gpu):
 # training and in evaluation alike: the network is trained on the cells of
 # one leaf size and does not carry over to another.
 LEAF = 256
+# The network's test runs at four cube widths: there the dipole far field
+# covers the cells nearest the near field, whose residual the network learns
+WIDTHS = 4.0
 
 
 def surrogate_rates(w, order, mlp=None):
     c = capi.Context(precision=capi.FP32C, nu=1e-4)
     k = c.add_wake(w.n)
     c.set_particles(k, w)
-    c.surrogate_enable(order=order, use_mlp=1 if mlp is not None else 0, check_targets=0, leaf_size=LEAF)
+    c.surrogate_enable(order=order, use_mlp=1 if mlp is not None else 0, check_targets=0, leaf_size=LEAF,
+                       near_widths=WIDTHS)
     if mlp is not None:
         c.surrogate_set_mlp(mlp)
     c.solve()
@@ -108,7 +112,7 @@ def training_set(mlp, n_per_case=200_000):
         c.set_particles(k, w)
         # the 5000-particle ring has far cells only with small leaves; the
         # features are scale-free, so samples of any leaf size mix
-        c.surrogate_enable(order=1, check_targets=0, leaf_size=32 if w.n < 20_000 else LEAF)
+        c.surrogate_enable(order=1, check_targets=0, leaf_size=32 if w.n < 20_000 else LEAF, near_widths=WIDTHS)
         c.solve()
         mlp.add_samples(c, n_per_case, seed=i)
         c.close()
