@@ -103,6 +103,8 @@ def parse():
     ap.add_argument("--kernel", choices=["gaussian", "highorder"], default="gaussian")
     ap.add_argument("--omega", type=float, default=1.0, help="rotor angular speed (dt = 10 deg / omega)")
     ap.add_argument("--mlp-steps", type=int, default=20)
+    ap.add_argument("--report-every", type=int, default=0, help="rotor: a progress line every this many steps")
+    ap.add_argument("--split", action="store_true", help="rotor: split FP32 positions (pgpu_config.split_positions)")
     a = ap.parse_args()
     if a.stations is None:
         a.stations = 200 if a.case else N_STATIONS
@@ -565,16 +567,22 @@ def run_shard(args):
     w = workload(args.stations)
     n = w.n
     b = shard.GpuShard(w, rank, world, precision=capi.FP32C, nu=NU, device=local)
-    stepper = shard.ShardedStepper(b, shard.DistExchange(b))
+    exchange = shard.DistExchange(b)
+    stepper = shard.ShardedStepper(b, exchange)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
     shape, _ = b.ctx.autotune(reps=1)  # over this rank's owned targets (untimed)
+    b.ctx.pair_kernel_time()
+    b.ctx.pair_counts()
+    # eager warm-up steps: the pair kernel's device time and pair counts (the
+    # graph replays below run with the library's timing off)
     for _ in range(args.warmup):
         stepper.step("rk4", DT, 1)
     torch.cuda.synchronize()
-    b.ctx.pair_kernel_time()
-    b.ctx.pair_counts()
+    pair_ms, pair_launches = b.ctx.pair_kernel_time()
+    pairs_timed, full_timed = b.ctx.pair_counts()
+    graphed = shard.GraphedStepper(b, exchange, "rk4", DT)
+    graphed.step(1)  # first replay (untimed)
     clocks = ClockSampler(local)
-    launches0 = b.ctx.launch_count()
     dist.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -584,16 +592,15 @@ def run_shard(args):
             with torch.cuda.stream(b.stream):
                 flush.zero_()
         ev0.record(b.stream)
-        stepper.step("rk4", DT, 1)
+        graphed.step(1)
         ev1.record(b.stream)
         ev1.synchronize()
         step_ms += ev0.elapsed_time(ev1)
     torch.cuda.synchronize()
     dist.barrier()
     clk = clocks.stop()
-    launches = b.ctx.launch_count() - launches0
-    pair_ms, pair_launches = b.ctx.pair_kernel_time()
-    pairs_timed, full_timed = b.ctx.pair_counts()
+    # per replayed step: per stage one box, one pair and one stage launch
+    launches = args.steps * 4 * 3
     t = torch.tensor([step_ms], dtype=torch.float64, device=f"cuda:{local}")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     step_ms = float(t.item())
@@ -615,7 +622,7 @@ def run_shard(args):
         e0.record(b.stream)
         for _ in range(args.steps):
             b.ctx.set_particles(b.wake, host)
-            stepper.step("rk4", DT, 1)
+            graphed.step(1)
             b.ctx.state(b.wake, out=(opos, oalpha))
         e1.record(b.stream)
         e1.synchronize()
@@ -636,6 +643,7 @@ def run_shard(args):
             "config": {"workload": WORKLOAD, "particles": n, "parallelism": f"targets{world}",
                        "pair_kernel_shape": {"block": shape[0], "targets_per_thread": shape[1]},
                        "exchange": f"NCCL all-gather of the FP32 source records after each RK stage ({32 * n} B)",
+                       "step": "stages and all-gathers of one RK4 step replayed from one CUDA graph",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "precision": "FP32 pairs, compensated sums, FP64 state"},
             "pair_interactions_per_s": 4 * n * (n - 1) * steps_per_s,
@@ -649,6 +657,7 @@ def run_shard(args):
             "clocks": clk,
         }
         print(json.dumps(out))
+    graphed.close()  # the graph holds NCCL calls: released before the process group
     b.close()
     dist.destroy_process_group()
 
@@ -757,9 +766,12 @@ def run_case(a) -> None:
     else:
         sh = cases.RotorShedder(omega=a.omega)
         cap = 4 * sh.per_blade * (steps + 1)
-        with capi.Context(precision=capi.FP32C, nu=NU, vinf=sh.inflow) as c:
+        with capi.Context(precision=capi.FP32C, nu=NU, vinf=sh.inflow, split_positions=a.split) as c:
             k = c.add_wake(cap)
-            c.set_particles(k, sh.shed())
+            first = sh.shed()
+            c.set_particles(k, first)
+            shed_sum = first.alpha.sum(axis=0)
+            shed_abs = np.abs(first.alpha).sum()
             pairs = 0
             t0 = time.perf_counter()
             t_last = t0
@@ -770,7 +782,21 @@ def run_case(a) -> None:
                     c.sync()
                     t_last = time.perf_counter()
                 c.step("rk3", sh.dt, 1)
-                c.append_particles(k, sh.shed())
+                new = sh.shed()
+                c.append_particles(k, new)
+                shed_sum += new.alpha.sum(axis=0)
+                shed_abs += np.abs(new.alpha).sum()
+                if a.report_every and (it + 1) % a.report_every == 0:
+                    c.sync()
+                    _, alpha = c.state(k)
+                    # stretching and diffusion are antisymmetric in each pair:
+                    # the total strength equals the sum of the shed strengths
+                    drift = float(np.abs(alpha.sum(axis=0) - shed_sum).max() / shed_abs)
+                    print(json.dumps({"step": it + 1, "particles": c.num_particles(k),
+                                      "elapsed_s": time.perf_counter() - t0, "pairs": pairs,
+                                      "pairs_per_s": pairs / (time.perf_counter() - t0),
+                                      "total_vorticity_drift": drift,
+                                      "max_alpha": float(np.linalg.norm(alpha, axis=1).max())}), flush=True)
             c.sync()
             t1 = time.perf_counter()
             n_end = c.num_particles(k)

@@ -94,18 +94,38 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// Byte offset of element (r, k) of a no-swizzle K-major tile with `rows` rows
-// (a multiple of 8) and 64 columns of BF16.
+// Byte offset of element (r, k) of a no-swizzle tile with `rows` rows (a
+// multiple of 8) and 64 columns of BF16, in core matrices of 8 x 8 elements
+// (128 contiguous bytes) stacked along the rows every 128 B and along K every
+// rows x 16 B.  K-major: a core matrix row holds 8 consecutive k of one r;
+// MN-major: 8 consecutive r of one k.  The descriptors of both take the same
+// offsets (LBO = rows x 16 B between K groups, SBO = 128 B between row groups).
 __device__ __forceinline__ int kmajor_off(int r, int k, int rows) {
   return (r & 7) * 16 + (r >> 3) * 128 + (k >> 3) * (rows * 16) + (k & 7) * 2;
 }
-
-// op(A) element (m, k) and op(B) element (k, n) as GemmArgs defines them.
-__device__ __forceinline__ float tc_a(const GemmArgs &g, int m, int k) {
-  return g.transA ? g.A[(int64_t)k * g.lda + m] : g.A[(int64_t)m * g.lda + k];
+__device__ __forceinline__ int mnmajor_off(int r, int k, int rows) {
+  return (k & 7) * 16 + (r >> 3) * 128 + (k >> 3) * (rows * 16) + (r & 7) * 2;
 }
-__device__ __forceinline__ float tc_b(const GemmArgs &g, int k, int n) {
-  return g.transB ? g.B[(int64_t)n * g.ldb + k] : g.B[(int64_t)k * g.ldb + n];
+
+// Eight consecutive FP32 values of a row of `src` (leading dimension ld)
+// starting at column c, zero where the row or a column is out of range
+// (vector loads when the run is whole and 16-byte aligned), as BF16.
+__device__ __forceinline__ uint4 load8_bf16(const float *src, int64_t ld, int row, int nrows, int c, int ncols) {
+  float v[8];
+  const float *p = src + (int64_t)row * ld + c;
+  if (row < nrows && c + 8 <= ncols && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+    const float4 a = *reinterpret_cast<const float4 *>(p), b = *reinterpret_cast<const float4 *>(p + 4);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = (row < nrows && c + j < ncols) ? p[j] : 0.f;
+  }
+  uint4 o;
+  o.x = pack_bf16(v[0], v[1]);
+  o.y = pack_bf16(v[2], v[3]);
+  o.z = pack_bf16(v[4], v[5]);
+  o.w = pack_bf16(v[6], v[7]);
+  return o;
 }
 
 // Dynamic shared memory of a CTA: the two operand tiles, padded so that at
@@ -138,25 +158,40 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, int *err) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = s_tmem;
-  constexpr uint32_t idesc = umma_idesc_bf16(kTcBM, BN);
+  // Each operand is staged in the major order of its global layout, 16 bytes
+  // (8 BF16) per store: op(A) is K-major unless A is transposed (then its M
+  // run is contiguous: MN-major, idesc bit 15); op(B) is K-major when B is
+  // transposed, else N-major (idesc bit 16).
+  const uint32_t idesc =
+      umma_idesc_bf16(kTcBM, BN) | ((g.transA ? 1u : 0u) << 15) | ((g.transB ? 0u : 1u) << 16);
   uint32_t phase = 0;
   bool ok = true;
   int issued = 0;
   for (int k0 = kz0; k0 < kz1; k0 += kTcBK) {
     const int kc = min(kTcBK, kz1 - k0);
-    // op(A) tile: consecutive threads take consecutive elements of the
-    // contiguous global dimension (k, or m when A is transposed)
-    for (int i = tid; i < kTcBM * kTcBK; i += 128) {
-      const int m = g.transA ? (i & (kTcBM - 1)) : (i >> 6);
-      const int k = g.transA ? (i >> 7) : (i & (kTcBK - 1));
-      const float v = (m0 + m < g.M && k < kc) ? tc_a(g, m0 + m, k0 + k) : 0.f;
-      *reinterpret_cast<__nv_bfloat16 *>(sA + kmajor_off(m, k, kTcBM)) = __float2bfloat16_rn(v);
+    // op(A) tile, 1024 runs of 8: consecutive threads take consecutive runs
+    // along the contiguous global dimension
+    for (int i = tid; i < kTcBM * kTcBK / 8; i += 128) {
+      if (!g.transA) {
+        const int m = i >> 3, kg = i & 7;  // A[m][k], k contiguous
+        *reinterpret_cast<uint4 *>(sA + kmajor_off(m, 8 * kg, kTcBM)) =
+            load8_bf16(g.A, g.lda, m0 + m, g.M, k0 + 8 * kg, kz1);
+      } else {
+        const int k = i >> 4, mg = i & 15;  // A[k][m], m contiguous
+        *reinterpret_cast<uint4 *>(sA + mnmajor_off(8 * mg, k, kTcBM)) =
+            load8_bf16(g.A, g.lda, k0 + k, kz1, m0 + 8 * mg, g.M);
+      }
     }
-    for (int i = tid; i < BN * kTcBK; i += 128) {
-      const int n = g.transB ? (i >> 6) : (i % BN);
-      const int k = g.transB ? (i & (kTcBK - 1)) : (i / BN);
-      const float v = (n0 + n < g.N && k < kc) ? tc_b(g, k0 + k, n0 + n) : 0.f;
-      *reinterpret_cast<__nv_bfloat16 *>(sB + kmajor_off(n, k, BN)) = __float2bfloat16_rn(v);
+    for (int i = tid; i < BN * kTcBK / 8; i += 128) {
+      if (g.transB) {
+        const int n = i >> 3, kg = i & 7;  // B[n][k], k contiguous
+        *reinterpret_cast<uint4 *>(sB + kmajor_off(n, 8 * kg, BN)) =
+            load8_bf16(g.B, g.ldb, n0 + n, g.N, k0 + 8 * kg, kz1);
+      } else {
+        const int k = i / (BN / 8), ng = i % (BN / 8);  // B[k][n], n contiguous
+        *reinterpret_cast<uint4 *>(sB + mnmajor_off(8 * ng, k, BN)) =
+            load8_bf16(g.B, g.ldb, k0 + k, kz1, n0 + 8 * ng, g.N);
+      }
     }
     // the generic-proxy stores must be visible to the tensor cores' async proxy
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -199,23 +234,37 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(GemmArgs g, int *err) {
         for (int j = 0; j < 16; ++j) v[j] = 0.f;
       }
       if (m < g.M) {
+        const int nb = n0 + c;
+        const int64_t o0 = (int64_t)m * g.ldc + nb;
+        if (g.epi == kEpiAtomic) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int n = n0 + c + j;
-          if (n >= g.N) continue;
-          const int64_t o = (int64_t)m * g.ldc + n;
-          const float a = v[j];
-          switch (g.epi) {
-            case kEpiStore: g.C[o] = a; break;
-            case kEpiBias: g.C[o] = a + g.bias[n]; break;
-            case kEpiBiasGelu: {
-              const float z = a + g.bias[n];
-              g.C[o] = z;
-              g.H[o] = gelu_f(z);
-              break;
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < g.N) atomicAdd(g.C + o0 + j, v[j]);
+        } else {
+          float h[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int n = nb + j < g.N ? nb + j : g.N - 1;  // clamped: columns past N are not stored
+            if (g.epi == kEpiBias || g.epi == kEpiBiasGelu) v[j] += g.bias[n];
+            if (g.epi == kEpiBiasGelu) h[j] = gelu_f(v[j]);
+            if (g.epi == kEpiGeluGrad) v[j] *= gelu_grad(g.Z[(int64_t)m * g.ldc + n]);
+          }
+          const bool vec = nb + 16 <= g.N && ((reinterpret_cast<uintptr_t>(g.C + o0) & 15) == 0) &&
+                           (g.epi != kEpiBiasGelu || ((reinterpret_cast<uintptr_t>(g.H + o0) & 15) == 0));
+          if (vec) {
+#pragma unroll
+            for (int j = 0; j < 16; j += 4) {
+              *reinterpret_cast<float4 *>(g.C + o0 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+              if (g.epi == kEpiBiasGelu)
+                *reinterpret_cast<float4 *>(g.H + o0 + j) = make_float4(h[j], h[j + 1], h[j + 2], h[j + 3]);
             }
-            case kEpiGeluGrad: g.C[o] = a * gelu_grad(g.Z[o]); break;
-            default: atomicAdd(g.C + o, a); break;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              if (nb + j >= g.N) continue;
+              g.C[o0 + j] = v[j];
+              if (g.epi == kEpiBiasGelu) g.H[o0 + j] = h[j];
+            }
           }
         }
       }

@@ -168,6 +168,43 @@ class ShardedStepper:
                 self.exchange()
 
 
+class GraphedStepper:
+    """One GpuShard's RK step (stage launches and the NCCL all-gather after
+    each stage) captured once in a CUDA graph on the context's stream and
+    replayed per step.  The capture uses thread-local mode, so the process
+    group's own bookkeeping on other threads stays legal, and the library's
+    pair-kernel timing is switched off (timing reads events on the host).
+    Every rank captures and replays the same collectives in the same order.
+    Call close() before destroying the process group."""
+
+    def __init__(self, backend: "GpuShard", exchange: "DistExchange", scheme: str, dt: float):
+        self.b, self.scheme, self.dt = backend, scheme, dt
+        # the work plan and NCCL's communicator are set up outside the capture:
+        # a rate evaluation (the state does not move) and one exchange of the
+        # unchanged records
+        backend.ctx.solve()
+        exchange()
+        torch.cuda.synchronize(backend.device)
+        backend.ctx.set_timing(False)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=backend.stream, capture_error_mode="thread_local"):
+            for s in range(STAGES[scheme]):
+                backend.stage(scheme, s, dt)
+                exchange()
+
+    def step(self, nsteps: int = 1):
+        with torch.cuda.stream(self.b.stream):
+            for _ in range(nsteps):
+                self.graph.replay()
+
+    def close(self):
+        if self.graph is not None:
+            torch.cuda.synchronize(self.b.device)
+            self.graph.reset()
+            self.graph = None
+            self.b.ctx.set_timing(True)
+
+
 def gather_state(backends) -> tuple[np.ndarray, np.ndarray]:
     """Whole (pos, alpha) from the owned rows of local backends."""
     pos = alpha = None

@@ -125,3 +125,43 @@ def test_sharded_diagnostics_two_wakes(gpu, prec, tol):
     scale = abs(ref[12])
     assert np.all(np.abs(got - ref) / np.maximum(np.abs(ref), scale) < tol)
     assert np.abs(vbi - ref_vbi).max() <= tol * np.abs(ref_vbi).max()
+
+
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_graphed_shard_step_equals_eager(gpu, scheme):
+    """The CUDA-graph replay of one sharded step (stages + NCCL all-gathers,
+    world size 1) advances the state exactly as the eager stage-by-stage
+    step does."""
+    import os
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        w = cases.ring_gaussian(stations=10, per_section=1000, seed=2)
+        eager = shard.GpuShard(w, 0, 1, precision=capi.FP64, nu=1e-4)
+        graphed = shard.GpuShard(w, 0, 1, precision=capi.FP64, nu=1e-4)
+        shard.ShardedStepper(eager, shard.DistExchange(eager)).step(scheme, 0.005, 3)
+        g = shard.GraphedStepper(graphed, shard.DistExchange(graphed), scheme, 0.005)
+        g.step(3)
+        torch.cuda.synchronize()
+        pe, ae = eager.state()
+        pg, ag = graphed.state()
+        g.close()
+        eager.close()
+        graphed.close()
+        np.testing.assert_array_equal(pg, pe)
+        np.testing.assert_array_equal(ag, ae)
+    finally:
+        dist.destroy_process_group()
