@@ -296,7 +296,7 @@ int pgpu_autotune_classes(pgpu_ctx *ctx, int reps, const char *cache_path, pgpu_
  * system uses an octree: each target leaf's near field (cells closer than
  * near_widths cube widths, or with a particle within sqrt(far_u) sigma_ij of the leaf's)
  * is summed exactly with the direct kernel's terms,
- * and farther cells act through their multipole moments (order 0/1/2),
+ * and farther cells act through their multipole moments (order 0/1/2/3),
  * optionally corrected by the learned model of pgpu_surrogate_set_mlp.  After
  * every evaluation, check_targets sampled targets are recomputed by the direct
  * sum; if the max-norm relative error of the velocity or of dalpha/dt
@@ -305,7 +305,7 @@ int pgpu_autotune_classes(pgpu_ctx *ctx, int reps, const char *cache_path, pgpu_
 typedef struct pgpu_surrogate_config {
   int leaf_size;       /* particles per octree leaf, 1..512 (default 256) */
   double near_widths;  /* near field: cells closer than this many cube widths (default 5) */
-  int order;           /* far-field expansion: 0 monopole, 1 + dipole, 2 + quadrupole (default) */
+  int order;           /* far-field expansion: 0 monopole, 1 + dipole, 2 + quadrupole (default), 3 + octupole */
   int use_mlp;         /* add the learned correction to the far field of `order` (pgpu_surrogate_set_mlp) */
   double tolerance;    /* maximum relative error of the velocity and of dalpha/dt on the sampled targets
                           (default 1e-4) */

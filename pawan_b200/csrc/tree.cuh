@@ -22,7 +22,7 @@
 namespace pgpu {
 
 constexpr int kTreeLevels = 21;
-constexpr int kCellFloats = 40;
+constexpr int kCellFloats = 72;
 constexpr int kListStack = 256;
 // Smallest u = rho^2 / sigma_ij^2 between any particle of a far cell and any
 // of the target leaf (rho >= 4 sigma_ij).  At 4M particles on the coaxial
@@ -45,7 +45,9 @@ struct TreeCell {
 //   0-2 c, 3-5 A = sum alpha, 6-14 M[a][b] = sum alpha_a y_b,
 //   15-32 Q[a][bc] = sum alpha_a y_b y_c for bc in (00,01,02,11,12,22),
 //   33 R = max |y|, 34 w = cube width, 35-37 cube centre, 38 mean sigma^2/2,
-//   39 largest sigma^2/2.
+//   39 largest sigma^2/2,
+//   40-69 T[a][bcd] = sum alpha_a y_b y_c y_d for bcd in (000,001,002,011,012,
+//   022,111,112,122,222) (the third moments of the order-3 expansion), 70-71 0.
 struct CellData { float v[kCellFloats]; };
 
 __device__ __forceinline__ unsigned f2ord(float f) {
@@ -217,8 +219,8 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
     for (int k = 0; k < 7; ++k) t[k] = block_sum_d(s[k], red);
     const double cnt = (double)(c.end - c.start);
     const double cx = t[0] / cnt, cy = t[1] / cnt, cz = t[2] / cnt;
-    double m[27];
-    for (int k = 0; k < 27; ++k) m[k] = 0.0;
+    double m[57];
+    for (int k = 0; k < 57; ++k) m[k] = 0.0;
     float R = 0.f, H = 0.f;
     for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
       const float4 p = Ps[i], q = Qs[i];
@@ -234,10 +236,21 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
         m[9 + 6 * aa + 3] += a[aa] * y[1] * y[1];
         m[9 + 6 * aa + 4] += a[aa] * y[1] * y[2];
         m[9 + 6 * aa + 5] += a[aa] * y[2] * y[2];
+        double *o = m + 27 + 10 * aa;
+        o[0] += a[aa] * y[0] * y[0] * y[0];
+        o[1] += a[aa] * y[0] * y[0] * y[1];
+        o[2] += a[aa] * y[0] * y[0] * y[2];
+        o[3] += a[aa] * y[0] * y[1] * y[1];
+        o[4] += a[aa] * y[0] * y[1] * y[2];
+        o[5] += a[aa] * y[0] * y[2] * y[2];
+        o[6] += a[aa] * y[1] * y[1] * y[1];
+        o[7] += a[aa] * y[1] * y[1] * y[2];
+        o[8] += a[aa] * y[1] * y[2] * y[2];
+        o[9] += a[aa] * y[2] * y[2] * y[2];
       }
     }
-    double mt[27];
-    for (int k = 0; k < 27; ++k) mt[k] = block_sum_d(m[k], red);
+    double mt[57];
+    for (int k = 0; k < 57; ++k) mt[k] = block_sum_d(m[k], red);
     const float Rm = block_max_f(R, redf);
     const float Hm = block_max_f(H, redf);
     if (threadIdx.x == 0) {
@@ -255,6 +268,9 @@ __global__ void moments_kernel(const TreeCell *cells, int ncells, const float4 *
       d.v[37] = geo[2] + (iz + 0.5f) * w;
       d.v[38] = (float)(t[6] / cnt);
       d.v[39] = Hm;
+      for (int k = 0; k < 30; ++k) d.v[40 + k] = (float)mt[27 + k];
+      d.v[70] = 0.f;
+      d.v[71] = 0.f;
       out[ci] = d;
     }
     __syncthreads();

@@ -5,16 +5,19 @@
 // singular kernel, written with phi(d) = 1/|d| (4 pi units, as the pair kernel):
 //   velocity    alpha_s x d / rho^3                     = -alpha_s x grad phi(d)
 //   stretching  b/rho^3 - 3 (d.b) d / rho^5, b = alpha_t x alpha_s  = -D2(d) b
-// Expanding d = r - y about the cell centroid (r = x_t - c, y = x_s - c) to
-// second order in y, with A = sum alpha, M_ab = sum alpha_a y_b,
-// Q_abc = sum alpha_a y_b y_c and Dn the n-th derivative tensors of phi at r:
-//   u_i = -eps_iab [A_a D1_b - M_ac D2_bc + 1/2 Q_acd D3_bcd]
-//   s_i = -[D2_ik B_k - D3_ikc N_kc + 1/2 D4_ikcd P_kcd],
-//         B = alpha_t x A, N_.c = alpha_t x M_.c, P_.cd = alpha_t x Q_.cd.
-// `order` 0 keeps the monopole, 1 adds the dipole, 2 the quadrupole.  The
-// contractions below never form D3/D4; tests/test_surrogate.py checks the
-// result end to end (the order-2 far field reproduces the direct sum to
-// ~2e-5 on the leapfrogging rings, and the error falls with the order).
+// Expanding d = r - y about the cell centroid (r = x_t - c, y = x_s - c) in
+// powers of y, with A = sum alpha, M_ab = sum alpha_a y_b,
+// Q_abc = sum alpha_a y_b y_c, T_abcd = sum alpha_a y_b y_c y_d and Dn the
+// n-th derivative tensors of phi at r:
+//   u_i = -eps_iab [A_a D1_b - M_ac D2_bc + 1/2 Q_acd D3_bcd - 1/6 T_acde D4_bcde]
+//   s_i = -[D2_ik B_k - D3_ikc N_kc + 1/2 D4_ikcd P_kcd - 1/6 D5_ikcde R_kcde],
+//         B = alpha_t x A, N_.c = alpha_t x M_.c, P_.cd = alpha_t x Q_.cd,
+//         R_.cde = alpha_t x T_.cde.
+// `order` 0 keeps the monopole, 1 adds the dipole, 2 the quadrupole, 3 the
+// octupole.  The contractions below never form the derivative tensors; the
+// order-3 contractions were checked in a CPU restatement against the full
+// tensor contraction, and tests/test_surrogate.py checks the result end to
+// end (the error falls with the order against the direct sum).
 //
 // Near leaves.  Exact pair sums with the same three-regime FP32 terms as the
 // direct kernel.
@@ -120,6 +123,75 @@ __device__ __forceinline__ void far_expand(const float *v, const float *x, const
                       15.f * ir7 * (rPr[i] + 2.f * sumPk + 2.f * r[i] * sPrk + r[i] * rtr) +
                       3.f * ir5 * (trP[i] + 2.f * spik);
     s[i] -= 0.5f * d4p;
+  }
+  if (order < 3) return;
+  // ---- octupole; T_a packed (000,001,002,011,012,022,111,112,122,222).
+  // For a symmetric third-order tensor S: Sr[b][d] = S_bde r_e (symmetric),
+  // S1 = Sr r, S0 = S1.r, tS_b = S_bdd, and S_ccd r_d = tS.r.
+  //   u_i += 1/6 eps_iab [105 S0_a r_b / rho^9 - 45 (S1_ab + r_b (tS_a.r)) / rho^7 + 9 tS_ab / rho^5]
+  //   s_i += 1/6 D5_ikcde R_kcde, R_k = (alpha_t x T_.)_k, by the pairings of
+  //   D5 = -945 r r r r r / rho^11 + 105 sum_10 (delta r r r) / rho^9 - 15 sum_15 (delta delta r) / rho^7
+  const float ir11 = ir9 * ir2;
+  auto sym3 = [&](const float *S, float Sr[3][3], float *S1, float &S0, float *tS) {
+    // S index of (b, c, d), b <= c <= d sorted
+    Sr[0][0] = S[0] * r[0] + S[1] * r[1] + S[2] * r[2];
+    Sr[0][1] = S[1] * r[0] + S[3] * r[1] + S[4] * r[2];
+    Sr[0][2] = S[2] * r[0] + S[4] * r[1] + S[5] * r[2];
+    Sr[1][1] = S[3] * r[0] + S[6] * r[1] + S[7] * r[2];
+    Sr[1][2] = S[4] * r[0] + S[7] * r[1] + S[8] * r[2];
+    Sr[2][2] = S[5] * r[0] + S[8] * r[1] + S[9] * r[2];
+    Sr[1][0] = Sr[0][1]; Sr[2][0] = Sr[0][2]; Sr[2][1] = Sr[1][2];
+    for (int b = 0; b < 3; ++b) S1[b] = Sr[b][0] * r[0] + Sr[b][1] * r[1] + Sr[b][2] * r[2];
+    S0 = S1[0] * r[0] + S1[1] * r[1] + S1[2] * r[2];
+    tS[0] = S[0] + S[3] + S[5];
+    tS[1] = S[1] + S[6] + S[8];
+    tS[2] = S[2] + S[7] + S[9];
+  };
+  const float *Tp = v + 40;
+  {
+    float S0[3], S1[3][3], tS[3][3], Sr[3][3];
+    for (int a = 0; a < 3; ++a) sym3(Tp + 10 * a, Sr, S1[a], S0[a], tS[a]);
+    for (int i = 0; i < 3; ++i) {
+      const int a1 = (i + 1) % 3, b1 = (i + 2) % 3;  // eps_i a1 b1 = +1
+      const float x1 = 105.f * ir9 * (S0[a1] * r[b1] - S0[b1] * r[a1]);
+      const float sa1 = tS[a1][0] * r[0] + tS[a1][1] * r[1] + tS[a1][2] * r[2];
+      const float sb1 = tS[b1][0] * r[0] + tS[b1][1] * r[1] + tS[b1][2] * r[2];
+      const float x2 = -45.f * ir7 * ((S1[a1][b1] - S1[b1][a1]) + (sa1 * r[b1] - sb1 * r[a1]));
+      const float x3 = 9.f * ir5 * (tS[a1][b1] - tS[b1][a1]);
+      u[i] += (x1 + x2 + x3) * (1.f / 6.f);
+    }
+  }
+  {
+    // R_k = (alpha_t x T_.)_k, each a symmetric third-order tensor
+    float R[3][10];
+    for (int e = 0; e < 10; ++e) {
+      const float col[3] = {Tp[e], Tp[10 + e], Tp[20 + e]};
+      float p[3];
+      cross3f(at, col, p);
+      R[0][e] = p[0]; R[1][e] = p[1]; R[2][e] = p[2];
+    }
+    float M[3][3][3], r1[3][3], r0[3], tk[3][3];
+    for (int k = 0; k < 3; ++k) sym3(R[k], M[k], r1[k], r0[k], tk[k]);
+    float rr0 = 0.f, tr1 = 0.f, rsg = 0.f, trt = 0.f;
+    for (int k = 0; k < 3; ++k) {
+      rr0 += r[k] * r0[k];
+      tr1 += r1[k][k];
+      rsg += r[k] * (tk[k][0] * r[0] + tk[k][1] * r[1] + tk[k][2] * r[2]);
+      trt += tk[k][k];
+    }
+    for (int i = 0; i < 3; ++i) {
+      float rk1 = 0.f, rkt = 0.f, psi = 0.f;
+      for (int k = 0; k < 3; ++k) {
+        rk1 += r[k] * r1[k][i];
+        rkt += r[k] * tk[k][i];
+        psi += M[k][i][k];
+      }
+      const float ti_r = tk[i][0] * r[0] + tk[i][1] * r[1] + tk[i][2] * r[2];
+      const float t1 = -945.f * ir11 * r[i] * rr0;
+      const float t2 = 105.f * ir9 * (r0[i] + 3.f * rk1 + 3.f * r[i] * tr1 + 3.f * r[i] * rsg);
+      const float t3 = -15.f * ir7 * (3.f * r[i] * trt + 3.f * rkt + 3.f * ti_r + 6.f * psi);
+      s[i] += (t1 + t2 + t3) * (1.f / 6.f);
+    }
   }
 }
 
@@ -309,8 +381,10 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
     for (int c0 = 0; c0 < fn; c0 += kWarpCells) {
       const int cn = min(kWarpCells, fn - c0);
       __syncwarp();
-      for (int e = lane; e < cn * kCellFloats; e += 32)
-        ws.sc[e / kCellFloats][e % kCellFloats] = a.cd[a.far_list[fo + c0 + e / kCellFloats]].v[e % kCellFloats];
+      // the cell data the expansion reads: the third moments only at order 3
+      const int nf = a.order >= 3 ? kCellFloats : 40;
+      for (int e = lane; e < cn * nf; e += 32)
+        ws.sc[e / nf][e % nf] = a.cd[a.far_list[fo + c0 + e / nf]].v[e % nf];
       __syncwarp();
       float su[3] = {0, 0, 0}, ss[3] = {0, 0, 0};
       for (int j = 0; j < cn; ++j) {

@@ -49,13 +49,18 @@ def test_all_near_equals_direct(gpu, rings):
 
 def test_orders_converge_and_quadrupole_meets_gate(gpu, rings):
     vd, ad = direct(rings)
-    errs = []
-    for order in (0, 1, 2):
-        v, a, st = surrogate(rings, order=order, check_targets=0)
+    errs, derrs = [], []
+    for order in (0, 1, 2, 3):
+        # four cube widths, where the truncation error is largest
+        v, a, st = surrogate(rings, order=order, check_targets=0, near_widths=4.0)
         errs.append(O.rel_err(v, vd))
+        derrs.append(O.rel_err(a, ad))
         assert st["fallbacks"] == 0
+    print("velocity / dalpha errors by order:", [f"{e:.2e}/{d:.2e}" for e, d in zip(errs, derrs)])
     assert errs[2] < errs[0]
     assert errs[2] < 1e-4, errs
+    # the octupole lowers both errors further
+    assert errs[3] < errs[2] and derrs[3] < derrs[2], (errs, derrs)
 
 
 def test_sampled_gate_reports_error(gpu, rings):
