@@ -223,6 +223,35 @@ int pgpu_diagnose_combine(const double *fields, int32_t nwakes, double zc_prev, 
  * (npts, 3)) by every particle of a system, using each particle's own radius. */
 int pgpu_probe(pgpu_ctx *ctx, int32_t system, int64_t npts, const double *pts, double *vel);
 
+/* Asynchronous state download for per-step output: the .wake record that
+ * PAWAN's offline loop writes after every step (__integration::integrate,
+ * integration.cpp:42-50, through __interaction::write, interaction.cpp:304-319,
+ * and __wake::write, wake.cpp:832-841).
+ *
+ * pgpu_snapshot_begin queues on the context's stream, after the work queued so
+ * far, a gather of every wake's positions and strengths into device buffer
+ * `slot` (0 or 1), then a device-to-host copy of that buffer into a pinned
+ * host buffer owned by the context, on a second stream, and returns without
+ * waiting.  Work queued afterwards (the next step) runs while the copy is in
+ * flight.  Before the gather overwrites a slot, the device waits for that
+ * slot's previous copy; the caller must have finished reading the slot's host
+ * buffer before it begins the slot again.
+ *
+ * pgpu_snapshot_wait blocks until the slot's copy has landed (PGPU_ETIMEOUT
+ * after `seconds`, the copy left running; seconds <= 0 waits without limit)
+ * and returns the host buffer in *state.  Wake w of the snapshot (in creation
+ * order) holds n[w] positions, row-major (n[w], 3), at *state + 6 * off[w],
+ * followed by its n[w] strengths, row-major (n[w], 3).  off and n receive up
+ * to `nwakes` entries (either may be NULL).  The buffer stays valid until the
+ * slot's next pgpu_snapshot_begin or pgpu_destroy.  Under a target range
+ * (pgpu_set_target_range) only the owned rows of the state are advanced by
+ * this context, and only those rows of a snapshot are current.
+ * Buffers: 6 * (total capacity) doubles per slot, on the device and pinned on
+ * the host, allocated by the slot's first begin. */
+int pgpu_snapshot_begin(pgpu_ctx *ctx, int32_t slot);
+int pgpu_snapshot_wait(pgpu_ctx *ctx, int32_t slot, double seconds, const double **state, int64_t *off, int64_t *n,
+                       int32_t nwakes);
+
 /* Waits for all queued work; reports PGPU_ENUMERIC if a step produced a
  * non-finite state. */
 int pgpu_sync(pgpu_ctx *ctx);

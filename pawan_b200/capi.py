@@ -43,7 +43,7 @@ EXPORTS = [
     "pgpu_mlp_dataset_rows", "pgpu_mlp_get_dataset", "pgpu_mlp_train", "pgpu_surrogate_set_mlp",
     "pgpu_rates_noalloc", "pgpu_noalloc_last_error", "pgpu_set_target_range", "pgpu_stage", "pgpu_records",
     "pgpu_sync_timeout", "pgpu_set_timing", "pgpu_influence", "pgpu_get_vorticity_field", "pgpu_merge",
-    "pgpu_get_particles",
+    "pgpu_get_particles", "pgpu_snapshot_begin", "pgpu_snapshot_wait",
 ]
 
 
@@ -169,6 +169,8 @@ def load(build_if_missing: bool = False):
         "pgpu_get_vorticity_field": (C.c_int, [vp, C.c_int32, _dp]),
         "pgpu_merge": (C.c_int, [vp, C.c_int32, C.c_int64, _i64p]),
         "pgpu_get_particles": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp, _dp]),
+        "pgpu_snapshot_begin": (C.c_int, [vp, C.c_int32]),
+        "pgpu_snapshot_wait": (C.c_int, [vp, C.c_int32, C.c_double, C.POINTER(_dp), _i64p, _i64p, C.c_int32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -356,6 +358,31 @@ class Context:
             self._ck(self.lib.pgpu_sync(self.h))
         else:
             self._ck(self.lib.pgpu_sync_timeout(self.h, float(timeout)))
+
+    def snapshot_begin(self, slot: int):
+        """Queues an asynchronous download of every wake's positions and
+        strengths into snapshot `slot` (0 or 1) and returns at once; work
+        queued afterwards overlaps the copy (pgpu_snapshot_begin)."""
+        self._ck(self.lib.pgpu_snapshot_begin(self.h, int(slot)))
+
+    def snapshot_wait(self, slot: int, timeout: float = 0.0) -> list[tuple[np.ndarray, np.ndarray]]:
+        """Waits for snapshot `slot` (PgpuError(PGPU_ETIMEOUT) after `timeout`
+        seconds if > 0) and returns per wake (positions (n, 3), strengths (n, 3)),
+        copied out of the context's pinned buffer."""
+        nw = len(self.wake_sizes)
+        state = _dp()
+        off = np.zeros(max(nw, 1), dtype=np.int64)
+        n = np.zeros(max(nw, 1), dtype=np.int64)
+        self._ck(self.lib.pgpu_snapshot_wait(self.h, int(slot), float(timeout), C.byref(state),
+                                             off.ctypes.data_as(_i64p), n.ctypes.data_as(_i64p), nw))
+        total = int((off[:nw] + n[:nw]).max()) if nw else 0
+        buf = np.ctypeslib.as_array(state, shape=(6 * total,)) if total else np.zeros(0)
+        out = []
+        for w in range(nw):
+            o, m = int(off[w]), int(n[w])
+            out.append((buf[6 * o: 6 * o + 3 * m].reshape(m, 3).copy(),
+                        buf[6 * o + 3 * m: 6 * o + 6 * m].reshape(m, 3).copy()))
+        return out
 
     def merge(self, wake: int, n_elig: int) -> int:
         """PAWAN's particle merge (__wake::merge) over the wake's first n_elig

@@ -127,6 +127,16 @@ struct pgpu_ctx {
   std::vector<cudaGraph_t> graph_defs;
   std::string err;
   SurrogateState *sur = nullptr;  // far-field surrogate of the single system, when enabled
+  // State snapshots (pgpu_snapshot_begin / _wait): per slot a device buffer,
+  // a pinned host buffer, the gather's and the copy's events, and the wake
+  // rows the snapshot holds.
+  cudaStream_t st_copy = nullptr;
+  double *d_snap[2] = {nullptr, nullptr};
+  double *h_snap[2] = {nullptr, nullptr};
+  cudaEvent_t snap_gathered[2] = {nullptr, nullptr};
+  cudaEvent_t snap_copied[2] = {nullptr, nullptr};
+  bool snap_begun[2] = {false, false};
+  std::vector<int64_t> snap_off[2], snap_n[2];
 };
 
 namespace {
@@ -630,6 +640,14 @@ int pgpu_destroy(pgpu_ctx *c) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 8; ++k) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
+  if (c->st_copy) cudaStreamSynchronize(c->st_copy);
+  for (int s = 0; s < 2; ++s) {
+    if (c->d_snap[s]) cudaFree(c->d_snap[s]);
+    if (c->h_snap[s]) cudaFreeHost(c->h_snap[s]);
+    if (c->snap_gathered[s]) cudaEventDestroy(c->snap_gathered[s]);
+    if (c->snap_copied[s]) cudaEventDestroy(c->snap_copied[s]);
+  }
+  if (c->st_copy) cudaStreamDestroy(c->st_copy);
   cudaStreamDestroy(c->st);
   delete c;
   return PGPU_OK;
@@ -1065,6 +1083,89 @@ int pgpu_sync_timeout(pgpu_ctx *c, double seconds) {
     std::this_thread::sleep_for(std::chrono::microseconds(100));
   }
   return pgpu_sync(c);
+}
+
+int pgpu_snapshot_begin(pgpu_ctx *c, int32_t slot) {
+  NvtxRange nvtx("pgpu_snapshot_begin");
+  if (!c) return PGPU_EINVAL;
+  if (slot != 0 && slot != 1) return fail(c, PGPU_EINVAL, "snapshot slot %d is not 0 or 1", slot);
+  if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
+  if (c->capturing) return fail(c, PGPU_EINVAL, "a snapshot cannot be taken during graph capture");
+  const size_t bytes = 6 * (size_t)c->cap * sizeof(double);
+  if (!c->st_copy) CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
+  if (!c->d_snap[slot]) {
+    if (cudaMalloc(&c->d_snap[slot], std::max<size_t>(bytes, 64)) != cudaSuccess) {
+      cudaGetLastError();
+      c->d_snap[slot] = nullptr;
+      return fail(c, PGPU_ENOMEM, "snapshot buffer of %zu bytes", bytes);
+    }
+    if (cudaHostAlloc(reinterpret_cast<void **>(&c->h_snap[slot]), std::max<size_t>(bytes, 64), cudaHostAllocDefault) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      c->h_snap[slot] = nullptr;
+      cudaFree(c->d_snap[slot]);
+      c->d_snap[slot] = nullptr;
+      return fail(c, PGPU_ENOMEM, "pinned snapshot buffer of %zu bytes", bytes);
+    }
+    CK(cudaEventCreateWithFlags(&c->snap_gathered[slot], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->snap_copied[slot], cudaEventDisableTiming));
+  }
+  // the gather must not overwrite the slot while its previous copy reads it
+  if (c->snap_begun[slot]) CK(cudaStreamWaitEvent(c->st, c->snap_copied[slot], 0));
+  auto &offs = c->snap_off[slot];
+  auto &ns = c->snap_n[slot];
+  offs.assign(c->wakes.size(), 0);
+  ns.assign(c->wakes.size(), 0);
+  int64_t total = 0;
+  for (size_t w = 0; w < c->wakes.size(); ++w) {
+    const WakeRec &W = c->wakes[w];
+    offs[w] = total;
+    ns[w] = W.n;
+    if (W.n > 0) {
+      const int grid = (int)std::min<int64_t>(ceil_div(W.n, 256), 16LL * c->sms);
+      gather_kernel<<<grid, 256, 0, c->st>>>(c->x0, W.n, W.off, c->cap, c->d_snap[slot] + 6 * total);
+      CK(cudaGetLastError());
+      c->launches++;
+    }
+    total += W.n;
+  }
+  CK(cudaEventRecord(c->snap_gathered[slot], c->st));
+  CK(cudaStreamWaitEvent(c->st_copy, c->snap_gathered[slot], 0));
+  if (total > 0)
+    CK(cudaMemcpyAsync(c->h_snap[slot], c->d_snap[slot], 6 * (size_t)total * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->st_copy));
+  CK(cudaEventRecord(c->snap_copied[slot], c->st_copy));
+  c->snap_begun[slot] = true;
+  return PGPU_OK;
+}
+
+int pgpu_snapshot_wait(pgpu_ctx *c, int32_t slot, double seconds, const double **state, int64_t *off, int64_t *n,
+                       int32_t nwakes) {
+  NvtxRange nvtx("pgpu_snapshot_wait");
+  if (!c) return PGPU_EINVAL;
+  if (slot != 0 && slot != 1) return fail(c, PGPU_EINVAL, "snapshot slot %d is not 0 or 1", slot);
+  if (!c->snap_begun[slot]) return fail(c, PGPU_EINVAL, "no snapshot was begun in slot %d", slot);
+  if (seconds > 0) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      const cudaError_t e = cudaEventQuery(c->snap_copied[slot]);
+      if (e == cudaSuccess) break;
+      if (e != cudaErrorNotReady) return fail(c, PGPU_ECUDA, "cudaEventQuery failed: %s", cudaGetErrorString(e));
+      const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (waited > seconds)
+        return fail(c, PGPU_ETIMEOUT, "snapshot %d did not land within %.3f s (the copy keeps running)", slot, seconds);
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+  } else {
+    CK(cudaEventSynchronize(c->snap_copied[slot]));
+  }
+  if (state) *state = c->h_snap[slot];
+  const int32_t m = std::min<int32_t>(std::max(nwakes, 0), (int32_t)c->snap_off[slot].size());
+  for (int32_t w = 0; w < m; ++w) {
+    if (off) off[w] = c->snap_off[slot][w];
+    if (n) n[w] = c->snap_n[slot][w];
+  }
+  return PGPU_OK;
 }
 
 int pgpu_pair_kernel_time(pgpu_ctx *c, double *ms, int64_t *launches) {

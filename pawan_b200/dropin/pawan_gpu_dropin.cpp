@@ -1,8 +1,12 @@
 // Drop-in GPU backend for PAWAN's C++ class surface (see pawan_gpu_dropin.h).
 #include "pawan_gpu_dropin.h"
 
+#include <string.h>
+
+#include <exception>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 namespace pawan {
 
@@ -87,6 +91,10 @@ void __gpu::solve() {
 // writediagnosis() emits.
 void __gpu::diagnose() {
   upload();
+  diagnose_on_device();
+}
+
+void __gpu::diagnose_on_device() {
   double out[15], vbi[3];
   check(pgpu_diagnose(_ctx, 0, out, vbi));
   for (int k = 0; k < 3; ++k) {
@@ -136,17 +144,105 @@ void __gpu::device_step(int scheme, double dt, int nsteps) {
   download_state();
 }
 
+void __gpu::write_snapshot(FILE *f, double t, int slot) {
+  const double *state = nullptr;
+  std::vector<int64_t> off(_wakes.size()), n(_wakes.size());
+  check(pgpu_snapshot_wait(_ctx, slot, 0.0, &state, off.data(), n.data(), (int32_t)_wakes.size()));
+  for (size_t k = 0; k < _wakes.size(); ++k) {
+    __wake *W = _wakes[k];
+    const int32_t id = _ids[k];
+    if ((size_t)n[id] != W->_numParticles) throw std::logic_error("pawan_gpu: wake size changed during integrate");
+    memcpy(W->_position->data, state + 6 * off[id], 3 * (size_t)n[id] * sizeof(double));
+    memcpy(W->_vorticity->data, state + 6 * off[id] + 3 * n[id], 3 * (size_t)n[id] * sizeof(double));
+  }
+  fwrite(&t, sizeof(double), 1, f);
+  write(f);  // __interaction::write (interaction.cpp:304-319)
+}
+
+// Per step: the device step, then (once the previous record is written, which
+// frees the slot used two steps ago) a snapshot into slot i % 2 handed to a
+// writer thread, then the diagnostics on the device.  The writer of step i
+// writes while step i + 1 computes.
+void __gpu::integrate_on_device(int scheme, double dt, size_t nsteps, __io *IO, bool diag) {
+  FILE *f = IO->create_binary_file(".wake");
+  FILE *fdiag = IO->create_binary_file(".diagnosis");
+  if (!f || !fdiag) {
+    if (f) fclose(f);
+    if (fdiag) fclose(fdiag);
+    throw std::runtime_error("pawan_gpu: cannot create the .wake / .diagnosis files");
+  }
+  std::thread writer;
+  std::exception_ptr werr;
+  auto join = [&] {
+    if (writer.joinable()) writer.join();
+    if (werr) {
+      std::exception_ptr e = werr;
+      werr = nullptr;
+      std::rethrow_exception(e);
+    }
+  };
+  try {
+    double t = 0.0;
+    fwrite(&t, sizeof(double), 1, f);
+    write(f);  // the initial particles as they are
+    if (diag) {
+      writenu(fdiag);
+      fwrite(&t, sizeof(double), 1, fdiag);
+      diagnose();  // uploads the host wakes
+      writediagnosis(fdiag);
+    } else {
+      upload();
+    }
+    const double tStart = TIME();
+    for (size_t i = 1; i <= nsteps; ++i) {
+      OUT("\tStep", i);
+      t = i * dt;
+      check(pgpu_step(_ctx, scheme, dt, 1));
+      join();
+      const int slot = (int)(i & 1);
+      check(pgpu_snapshot_begin(_ctx, slot));
+      writer = std::thread([this, f, t, slot, &werr] {
+        try {
+          write_snapshot(f, t, slot);
+        } catch (...) {
+          werr = std::current_exception();
+        }
+      });
+      if (diag) {
+        diagnose_on_device();
+        fwrite(&t, sizeof(double), 1, fdiag);
+        writediagnosis(fdiag);
+      }
+    }
+    join();
+    check(pgpu_sync(_ctx));
+    OUT("Total Time (s)", TIME() - tStart);
+  } catch (...) {
+    if (writer.joinable()) writer.join();
+    fclose(f);
+    fclose(fdiag);
+    throw;
+  }
+  fclose(f);
+  fclose(fdiag);
+}
+
 void __gpu::probe(const double *pts, long npts, double *vel) {
   upload();
   check(pgpu_probe(_ctx, 0, (int64_t)npts, pts, vel));
+}
+
+static __gpu *gpu_system(__system *S) {
+  __gpu *G = dynamic_cast<__gpu *>(S);
+  if (!G) throw std::invalid_argument("pawan_gpu: a GPU integrator needs a pawan::__gpu system");
+  return G;
 }
 
 // __rk4::step / __rk3::step (rk4.cpp:12-77, rk3.cpp:12-65): the stage loop
 // runs on the device.  On return `state` and the wakes hold the new state, as
 // after PAWAN's own step.
 static void gpu_step(int scheme, const double &dt, __system *S, gsl_vector *state) {
-  __gpu *G = dynamic_cast<__gpu *>(S);
-  if (!G) throw std::invalid_argument("pawan_gpu: a GPU integrator needs a pawan::__gpu system");
+  __gpu *G = gpu_system(S);
   S->setStates(state);
   G->device_step(scheme, dt, 1);
   S->getStates(state);
@@ -154,5 +250,12 @@ static void gpu_step(int scheme, const double &dt, __system *S, gsl_vector *stat
 
 void __rk4gpu::step(const double &dt, __system *S, gsl_vector *state) { gpu_step(PGPU_RK4, dt, S, state); }
 void __rk3gpu::step(const double &dt, __system *S, gsl_vector *state) { gpu_step(PGPU_RK3, dt, S, state); }
+
+void __rk4gpu::integrate(__system *S, __io *IO, bool diagnose) {
+  gpu_system(S)->integrate_on_device(PGPU_RK4, _dt, _n, IO, diagnose);
+}
+void __rk3gpu::integrate(__system *S, __io *IO, bool diagnose) {
+  gpu_system(S)->integrate_on_device(PGPU_RK3, _dt, _n, IO, diagnose);
+}
 
 }  // namespace pawan

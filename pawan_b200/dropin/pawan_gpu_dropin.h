@@ -11,6 +11,11 @@
  *     pawan::__integration *IN = new pawan::__rk4gpu(T, n);    // stages on the GPU
  *     IN->integrate(S, IO, true);                              // unchanged
  *
+ * Declaring IN as a pawan::__rk4gpu * (or __rk3gpu *) instead keeps the state
+ * on the device for the whole run and writes each step's .wake record from
+ * an asynchronous download while the next step computes
+ * (__gpu::integrate_on_device); the files are the same.
+ *
  * __gpu overrides the virtual members of __interaction that carry the hot
  * path (interaction.h:192-244): solve, diagnose, addWake, relax, and the
  * protected influence behind resolve().  Particle data stays
@@ -32,6 +37,8 @@
  */
 #ifndef PAWAN_GPU_DROPIN_H_
 #define PAWAN_GPU_DROPIN_H_
+
+#include <stdio.h>
 
 #include <vector>
 
@@ -72,6 +79,16 @@ class __gpu : public __interaction {
   // / PGPU_EULER) starting from the host wakes, then writes the new state back
   // into them.
   void device_step(int scheme, double dt, int nsteps);
+  // __integration::integrate (integration.cpp:24-60) with the state kept on
+  // the device from the first step to the last.  After each step an
+  // asynchronous snapshot (pgpu_snapshot_begin, two slots in turn) brings the
+  // state back while the next step runs, and a writer thread copies it into
+  // the host wakes and writes the step's .wake record with PAWAN's own
+  // __interaction::write; the diagnostics, when asked for, are computed on the
+  // device after each step and written with PAWAN's writediagnosis.  The
+  // .wake and .diagnosis files hold what PAWAN's loop writes, record for
+  // record, and the host wakes end at the final state.
+  void integrate_on_device(int scheme, double dt, size_t nsteps, __io *IO, bool diagnose);
   // Velocity induced at npts points (row-major) by all wakes, each particle
   // with its own radius (getVi, interaction.cpp:453-477).
   void probe(const double *pts, long npts, double *vel);
@@ -90,6 +107,10 @@ class __gpu : public __interaction {
   void layout();  // creates the device wakes on first use
   void upload();
   void download_state();
+  void diagnose_on_device();  // diagnose() without the upload of the host wakes
+  // Waits for snapshot `slot`, copies it into the host wakes and writes the
+  // .wake record of time t.
+  void write_snapshot(FILE *f, double t, int slot);
   pgpu_config _cfg;
   pgpu_ctx *_ctx = nullptr;
   std::vector<__wake *> _wakes;
@@ -97,9 +118,15 @@ class __gpu : public __interaction {
   bool _laid_out = false;
 };
 
+// integrate(S, IO, diagnose) called on a __rk4gpu / __rk3gpu (its static
+// type) runs __gpu::integrate_on_device.  Called through a pointer or
+// reference to __integration, PAWAN's own loop runs instead, with the GPU step
+// below and a synchronous download after each step: the same files either way.
 class __rk4gpu : public __rk4 {
  public:
   __rk4gpu(const double &t, const size_t &n) : __rk4(t, n) {}
+  using __rk4::integrate;
+  void integrate(__system *S, __io *IO, bool diagnose = false);
  protected:
   void step(const double &dt, __system *S, gsl_vector *state) override;
 };
@@ -107,6 +134,8 @@ class __rk4gpu : public __rk4 {
 class __rk3gpu : public __rk3 {
  public:
   __rk3gpu(const double &t, const size_t &n) : __rk3(t, n) {}
+  using __rk3::integrate;
+  void integrate(__system *S, __io *IO, bool diagnose = false);
  protected:
   void step(const double &dt, __system *S, gsl_vector *state) override;
 };

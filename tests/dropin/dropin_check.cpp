@@ -4,9 +4,14 @@
 // drop-in GPU classes (__gpu + __rk4gpu/__rk3gpu), writing <out>.wake and
 // <out>.diagnosis through PAWAN's own writers.
 //
-//   dropin_check ref|gpu|gpu64 rk4|rk3 <particles.bin> <dt> <nsteps> <out-prefix> [nu]
+//   dropin_check ref|gpu|gpu64|gpuasync|gpu64async rk4|rk3 <particles.bin> <dt> <nsteps> <out-prefix> [nu]
 //
 // particles.bin: int64 n, then n*3 positions, n*3 strengths, n radii, n volumes (FP64).
+// The *async modes call integrate on the __rk4gpu / __rk3gpu itself, which
+// keeps the state on the device and writes the .wake records from
+// asynchronous snapshots (__gpu::integrate_on_device); the others call it
+// through __integration *, PAWAN's own loop.  The wall time of integrate goes
+// to stderr as "integrate_seconds <s>".
 //
 // A second mode runs PAWAN's strength solve __resolve::rebuild
 // (src/resolve/resolve.cpp:12-63) on one of PAWAN's own __vring wakes
@@ -31,6 +36,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -203,6 +209,8 @@ int main(int argc, char **argv) {
   pawan::__interaction *S = nullptr;
   pawan::__integration *I = nullptr;
   const double T = dt * nsteps;
+  const bool async = mode.size() > 5 && mode.compare(mode.size() - 5, 5, "async") == 0;
+  const auto t0 = std::chrono::steady_clock::now();
   if (mode == "ref") {
     S = new ref_parallel(&W, nu);
     I = scheme == "rk3" ? (pawan::__integration *)new pawan::__rk3(T, nsteps) : new pawan::__rk4(T, nsteps);
@@ -210,13 +218,22 @@ int main(int argc, char **argv) {
     pgpu_config cfg;
     pgpu_config_default(&cfg);
     cfg.nu = nu;
-    cfg.precision = mode == "gpu64" ? PGPU_FP64 : PGPU_FP32C;
+    cfg.precision = mode.compare(0, 5, "gpu64") == 0 ? PGPU_FP64 : PGPU_FP32C;
     S = new pawan::__gpu(&W, cfg);
-    I = scheme == "rk3" ? (pawan::__integration *)new pawan::__rk3gpu(T, nsteps)
-                        : new pawan::__rk4gpu(T, nsteps);
+    if (scheme == "rk3") {
+      auto *R = new pawan::__rk3gpu(T, nsteps);
+      I = R;
+      if (async) R->integrate(S, &io, true);
+    } else {
+      auto *R = new pawan::__rk4gpu(T, nsteps);
+      I = R;
+      if (async) R->integrate(S, &io, true);
+    }
   }
-  I->integrate(S, &io, true);
+  if (!async) I->integrate(S, &io, true);
   fflush(NULL);
+  fprintf(stderr, "integrate_seconds %.6f\n",
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
   delete I;
   delete S;
   return 0;

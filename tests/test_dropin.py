@@ -102,6 +102,44 @@ def test_dropin_matches_reference_in_pawan_time_loop(gpu, driver, tmp_path, ref_
     np.testing.assert_allclose(dgot[:, 13:15], dref[:, 13:15], rtol=max(tol, 1e-10))
 
 
+def _mask_maxn_high(raw: bytes, nrec: int) -> bytearray:
+    """The .wake bytes with the undefined high half of each record's maxN
+    field zeroed (interaction.cpp:311-312 writes an int with sizeof(size_t))."""
+    b = bytearray(raw)
+    rec = len(b) // nrec
+    for k in range(nrec):
+        b[k * rec + 20: k * rec + 24] = b"\0\0\0\0"
+    return b
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,tol", [("gpu64", 1e-10), ("gpu", 1e-5)])
+@pytest.mark.parametrize("scheme", ["rk4", "rk3"])
+def test_device_resident_integrate_writes_the_same_files(gpu, driver, tmp_path, ref_available, mode, tol, scheme):
+    """__rk4gpu / __rk3gpu::integrate (state kept on the device, .wake records
+    from asynchronous snapshots written by a thread) against PAWAN's own loop
+    with the same GPU step: byte-identical .wake and .diagnosis files; and
+    against PAWAN's __parallel + __rk4/__rk3 at the mode's tolerance."""
+    g = np.load(GOLD / "ring1000.npz")
+    w = cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
+    nsteps = 6
+    ref, (_, dref) = run(driver, tmp_path, "ref", scheme, w, 0.01, nsteps)
+    sync, _ = run(driver, tmp_path, mode, scheme, w, 0.01, nsteps)
+    got, (nu, dgot) = run(driver, tmp_path, mode + "async", scheme, w, 0.01, nsteps)
+    assert len(got) == len(sync) == len(ref) == nsteps + 1
+    raw_sync = (tmp_path / f"{mode}_{scheme}.wake").read_bytes()
+    raw_async = (tmp_path / f"{mode}async_{scheme}.wake").read_bytes()
+    assert _mask_maxn_high(raw_async, nsteps + 1) == _mask_maxn_high(raw_sync, nsteps + 1)
+    assert (tmp_path / f"{mode}async_{scheme}.diagnosis").read_bytes() == \
+        (tmp_path / f"{mode}_{scheme}.diagnosis").read_bytes()
+    for (t0, a), (t1, b) in zip(got, ref):
+        assert t0 == t1
+        assert O.rel_err(a[0].pos, b[0].pos) < tol
+        assert O.rel_err(a[0].alpha, b[0].alpha) < tol
+    np.testing.assert_allclose(dgot[:, 4:10], dref[:, 4:10], rtol=max(tol, 1e-10),
+                               atol=max(tol, 1e-10) * np.abs(dref[:, 4:10]).max())
+
+
 def _resolve(driver, out, backend):
     r = subprocess.run([str(driver), "resolve", backend, "3", "49", "0.1924", str(out)],
                        capture_output=True, text=True, timeout=900)
