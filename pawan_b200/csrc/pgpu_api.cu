@@ -1107,11 +1107,12 @@ int pgpu_snapshot_begin(pgpu_ctx *c, int32_t slot) {
       c->d_snap[slot] = nullptr;
       return fail(c, PGPU_ENOMEM, "pinned snapshot buffer of %zu bytes", bytes);
     }
-    CK(cudaEventCreateWithFlags(&c->snap_gathered[slot], cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&c->snap_copied[slot], cudaEventDisableTiming));
   }
+  if (!c->snap_gathered[slot]) CK(cudaEventCreateWithFlags(&c->snap_gathered[slot], cudaEventDisableTiming));
+  if (!c->snap_copied[slot]) CK(cudaEventCreateWithFlags(&c->snap_copied[slot], cudaEventDisableTiming));
   // the gather must not overwrite the slot while its previous copy reads it
   if (c->snap_begun[slot]) CK(cudaStreamWaitEvent(c->st, c->snap_copied[slot], 0));
+  c->snap_begun[slot] = false;  // until this snapshot is fully queued
   auto &offs = c->snap_off[slot];
   auto &ns = c->snap_n[slot];
   offs.assign(c->wakes.size(), 0);
