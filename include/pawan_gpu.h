@@ -247,7 +247,12 @@ int pgpu_probe(pgpu_ctx *ctx, int32_t system, int64_t npts, const double *pts, d
  * (pgpu_set_target_range) only the owned rows of the state are advanced by
  * this context, and only those rows of a snapshot are current.
  * Buffers: 6 * (total capacity) doubles per slot, on the device and pinned on
- * the host, allocated by the slot's first begin. */
+ * the host, allocated by the slot's first begin.
+ * Threads: pgpu_snapshot_wait may run on another thread than the one queueing
+ * work on the context (a file writer), as long as no pgpu_snapshot_begin of
+ * the same slot runs at the same time; every other call on a context belongs
+ * to one thread at a time.  pgpu_last_error gives the message of whichever
+ * call failed last. */
 int pgpu_snapshot_begin(pgpu_ctx *ctx, int32_t slot);
 int pgpu_snapshot_wait(pgpu_ctx *ctx, int32_t slot, double seconds, const double **state, int64_t *off, int64_t *n,
                        int32_t nwakes);

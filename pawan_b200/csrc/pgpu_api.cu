@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <tuple>
@@ -125,7 +126,10 @@ struct pgpu_ctx {
   int64_t launches = 0;
   std::map<std::tuple<int, double, int, int, bool>, cudaGraphExec_t> graphs;  // (scheme, dt, launch layout, nch, timing)
   std::vector<cudaGraph_t> graph_defs;
-  std::string err;
+  // last error message: a fixed buffer under a mutex, since pgpu_snapshot_wait
+  // may fail on a writer thread while the owning thread queues work
+  char err[512] = {0};
+  std::mutex err_mu;
   SurrogateState *sur = nullptr;  // far-field surrogate of the single system, when enabled
   // State snapshots (pgpu_snapshot_begin / _wait): per slot a device buffer,
   // a pinned host buffer, the gather's and the copy's events, and the wake
@@ -154,7 +158,10 @@ int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
-  if (c) c->err = buf;
+  if (c) {
+    std::lock_guard<std::mutex> lock(c->err_mu);
+    memcpy(c->err, buf, sizeof(buf));
+  }
   return code;
 }
 
@@ -1545,7 +1552,7 @@ int pgpu_fp32_peak(int device, double *tflops, double *ms_out) {
   return PGPU_OK;
 }
 
-const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
+const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err : "null context"; }
 
 }  // extern "C"
 
