@@ -272,11 +272,12 @@ def time_steps(ctx, stream, scheme: str, dt: float, steps: int, flush=None) -> f
 # ------------------------------------------------------------------ sub-objects
 def run_fp64(w, device: int, fp64_peak: float) -> dict:
     """The headline ring stepped in the FP64 mode (FP64 pair terms and state),
-    one untimed and one timed RK4 step, shape 256 threads x 1 target (the FP64
-    kernel's fastest at 1M)."""
+    one untimed and one timed RK4 step, shape 128 threads x 1 target (the FP64
+    kernel's fastest at 1M: 3.09 s per evaluation against 3.22 s for 256 x 1
+    and 3.6 s or more for the two- and four-target shapes)."""
     import torch
     from pawan_b200 import capi
-    c = capi.Context(precision=capi.FP64, nu=NU, device=device, block=256, tpt=1)
+    c = capi.Context(precision=capi.FP64, nu=NU, device=device, block=128, tpt=1)
     k = c.add_wake(w.n)
     c.set_particles(k, w)
     stream = torch.cuda.ExternalStream(c.stream(), device=device)

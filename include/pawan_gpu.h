@@ -54,8 +54,8 @@ typedef struct pgpu_config {
   double nu;       /* kinematic viscosity (PAWAN's protected __interaction::_nu, interaction.h:25) */
   double vinf[3];  /* uniform inflow added after each step, x += vinf dt
                       (__wake::updateVinfEffect, wake.cpp:564-577, called from integration.cpp:172) */
-  int block;       /* pair-kernel threads per CTA; 0 = autotuned default */
-  int tpt;         /* pair-kernel targets per thread; 0 = autotuned default */
+  int block;       /* pair-kernel threads per CTA; 0 = default (Gaussian: 128; high-order: 256) until pgpu_autotune */
+  int tpt;         /* pair-kernel targets per thread; 0 = default (Gaussian FP32C: 2, FP64: 1; high-order: 1) */
   int chunks;      /* source chunks per system (1..16); 0 = automatic */
   int use_graphs;  /* capture each time step in a CUDA graph (default 1) */
   int kernel;      /* PGPU_KERNEL_GAUSSIAN (default) or PGPU_KERNEL_HIGHORDER; rates,

@@ -108,7 +108,7 @@ struct pgpu_ctx {
   int64_t pairs_acc = 0, selfs_acc = 0;  // ordered pairs and self pairs of the pair launches so far
   int *d_flag = nullptr;
   int diag_blocks = 0;
-  int shape = 2;  // (256, 1): the fastest shape at 1M particles before autotuning
+  int shape = 2;  // (256, 1) before autotuning: the high-order kernel's default (pgpu_create picks the Gaussian's)
   // Shapes per system chosen by pgpu_autotune_classes (empty: `shape` for
   // every system).  Each distinct shape in `groups` (ascending) is one pair
   // launch per evaluation over the systems that use it, with its own plan at
@@ -630,6 +630,11 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
       return PGPU_EINVAL;
     }
     c->shape = found;
+  } else if (c->cfg.kernel == PGPU_KERNEL_GAUSSIAN) {
+    // untuned defaults: the fastest Gaussian shapes on the 1M ring, FP32C
+    // 128 x 2 (1075 ms per evaluation against 1163 ms for 256 x 1) and FP64
+    // 128 x 1 (3.09 s against 3.22 s)
+    c->shape = c->cfg.precision == PGPU_FP32C ? 1 : 0;
   }
   *out = c;
   return PGPU_OK;
