@@ -140,7 +140,11 @@ int pgpu_step(pgpu_ctx *ctx, int scheme, double dt, int32_t nsteps);
  * the order of its wakes' particles); count < 0 restores all targets.  While
  * any system has a range, pgpu_step and pgpu_diagnose refuse (the state of
  * the other targets is not advanced here; pgpu_diagnose_partial gives this
- * context's share of the diagnostics), and the surrogate is off.
+ * context's share of the diagnostics).  With the surrogate enabled, every
+ * context builds the octree of the whole system from its (exchanged) records,
+ * evaluates only the tree's work items that hold owned targets, and draws its
+ * sampled check targets from the owned ones; its fallback is the direct sum
+ * over the owned targets.
  * pgpu_stage: stage 0..3 (RK4), 0..2 (RK3) or 0 (Euler) of one step of every
  * system; the last stage finishes the step (and applies vinf).
  * pgpu_records: device pointers to the system's source records, one per

@@ -527,6 +527,7 @@ int launch_pack(pgpu_ctx *c, int64_t lo, int64_t hi) {
 
 int surrogate_eval(pgpu_ctx *c);
 void surrogate_free(pgpu_ctx *c);
+int surrogate_pick_targets(pgpu_ctx *c, SurrogateState *s);
 
 int launch_eval(pgpu_ctx *c, int slot) {
   if (c->sur) return surrogate_eval(c);
@@ -799,7 +800,6 @@ int pgpu_solve(pgpu_ctx *c) {
 int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t count) {
   if (!c) return PGPU_EINVAL;
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
-  if (c->sur) return fail(c, PGPU_EINVAL, "the surrogate evaluates every target of its system");
   if (uses_split(c) && count >= 0)
     return fail(c, PGPU_EINVAL, "split positions are not exchanged between contexts: use one context per system");
   if (count >= 0 && first < 0) return fail(c, PGPU_EINVAL, "negative first target %lld", (long long)first);
@@ -807,6 +807,8 @@ int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t co
   S.t_first = count < 0 ? 0 : first;
   S.t_count = count < 0 ? -1 : count;
   c->plan_dirty = true;
+  // the surrogate's sampled check draws from the owned targets
+  if (c->sur) return surrogate_pick_targets(c, c->sur);
   return PGPU_OK;
 }
 
@@ -816,7 +818,6 @@ int pgpu_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
   if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
   if (stage < 0 || stage >= stages_of(scheme)) return fail(c, PGPU_EINVAL, "stage %d out of range for scheme %d", stage, scheme);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
-  if (c->sur) return fail(c, PGPU_EINVAL, "pgpu_stage runs the direct sum only; the surrogate steps with pgpu_step");
   int r = upload_plan(c);
   if (r) return r;
   if ((r = launch_eval(c, 0))) return r;

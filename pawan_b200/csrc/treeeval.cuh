@@ -316,6 +316,9 @@ struct TreeEvalArgs {
   int64_t cap;
   float nu2;
   int order;
+  // owned targets [own_lo, own_hi) (indices within the system); a context
+  // with a target range evaluates and writes only these
+  int own_lo, own_hi;
 };
 
 constexpr int kTreeBlock = 256;  // sampled-check kernel
@@ -373,6 +376,9 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
     const TreeCell tc = a.cells[a.leaves[li]];
     const int t0 = tc.start + it.y * 32 + lane;
     const int t = min(t0, tc.end - 1);
+    const int ti = a.idx[t];
+    const bool mine = t0 < tc.end && ti >= a.own_lo && ti < a.own_hi;
+    if (!__any_sync(0xffffffffu, mine)) continue;  // a slice with no owned target
     const float4 pt = a.Ps[t], qt = a.Qs[t];
     const float xt[3] = {pt.x, pt.y, pt.z}, at[3] = {qt.x, qt.y, qt.z};
     const float hst = pt.w, vt = qt.w;
@@ -556,8 +562,8 @@ __global__ void __launch_bounds__(32 * eval_warps<MLP>()) tree_eval_warp_kernel(
         }
       }
     }
-    if (t0 < tc.end) {
-      double *o = a.partial + a.off + a.idx[t0];
+    if (mine) {
+      double *o = a.partial + a.off + ti;
       for (int m = 0; m < 3; ++m) {
         o[m * a.cap] = ((double)vh[m] + (double)vl[m]) * kInv4Pi;
         o[(3 + m) * a.cap] = ((double)dh[m] + (double)dl[m]) * kInv4Pi;

@@ -46,8 +46,6 @@ def test_target_range_rules(gpu):
         with pytest.raises(capi.PgpuError, match="pgpu_diagnose_partial"):
             c.diagnose(0)
         with pytest.raises(capi.PgpuError):
-            c.surrogate_enable()
-        with pytest.raises(capi.PgpuError):
             c.stage("rk4", 4, 0.01)
         # rates of the owned targets only, equal to the full evaluation's
         c.solve()
@@ -165,3 +163,55 @@ def test_graphed_shard_step_equals_eager(gpu, scheme):
         np.testing.assert_array_equal(ag, ae)
     finally:
         dist.destroy_process_group()
+
+
+# The surrogate on a sharded system: every context builds the octree of the
+# whole system from its exchanged records and evaluates the work items that
+# hold its own targets.  A target's arithmetic does not depend on which
+# context owns it, so the sharded steps equal the unsharded surrogate steps
+# (bitwise; asserted at 1e-12).
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_surrogate_matches_unsharded(gpu, world):
+    w = cases.leapfrog_rings(n_total=60000)
+    kw = dict(tolerance=1.0, check_targets=512, leaf_size=64)
+    with capi.Context(precision=capi.FP32C, nu=1e-4) as c:
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        c.surrogate_enable(**kw)
+        c.step("rk4", 0.005, 2)
+        ref_pos, ref_alpha = c.state(k)
+        ref_stats = c.surrogate_stats()
+    bs = [shard.GpuShard(w, r, world, precision=capi.FP32C, nu=1e-4) for r in range(world)]
+    for b in bs:
+        b.ctx.surrogate_enable(**kw)
+    shard.ShardedStepper(bs, shard.LocalExchange(bs)).step("rk4", 0.005, 2)
+    pos, alpha = shard.gather_state(bs)
+    stats = [b.ctx.surrogate_stats() for b in bs]
+    for b in bs:
+        b.close()
+    assert ref_stats["evaluations"] == 8 and ref_stats["fallbacks"] == 0
+    for st in stats:
+        assert st["evaluations"] == 8 and st["fallbacks"] == 0
+        assert st["max_err_vel"] < 1e-4 and st["max_err_dalpha"] < 1e-4
+    assert O.rel_err(pos - w.pos, ref_pos - w.pos) < 1e-12
+    assert O.rel_err(alpha, ref_alpha) < 1e-12
+
+
+def test_sharded_surrogate_checks_owned_targets_and_falls_back(gpu):
+    """A rank's sampled check draws from its own targets; with a tolerance no
+    evaluation can meet, every evaluation falls back to the direct sum over
+    the owned targets, whose rates then equal the direct evaluation's."""
+    w = cases.leapfrog_rings(n_total=20000)
+    with capi.Context(precision=capi.FP32C, nu=1e-4) as c:
+        k = c.add_wake(w.n)
+        c.set_particles(k, w)
+        c.solve()
+        v_all, a_all = c.rates(k)
+        c.set_target_range(0, 5000, 8000)
+        c.surrogate_enable(tolerance=1e-30, check_targets=256)
+        c.solve()
+        st = c.surrogate_stats()
+        assert st["evaluations"] == 1 and st["fallbacks"] == 1
+        v, a = c.rates(k)
+        assert O.rel_err(v[5000:13000], v_all[5000:13000]) < 1e-6
+        assert O.rel_err(a[5000:13000], a_all[5000:13000]) < 1e-6
