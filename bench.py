@@ -24,7 +24,9 @@ packed FFMA2 register loop); `cpu_baseline` times PAWAN's own OpenMP code
 (compiled from its sources) on the host cores on a bounded sample and
 extrapolates quadratically to N.
 
-Sub-objects of the JSON line, measured after the headline timing on rank 0:
+Sub-objects of the JSON line, measured after the headline timing in a
+one-GPU run (N = 1; with N > 1 they and `cpu_baseline` are null, since they do
+not change with N and the other GPUs would wait idle):
 `fp64` (the same ring stepped in the FP64 mode, rated against the measured
 FP64 FMA peak), `diagnostics` (one pgpu_diagnose of the ring), `uneven64` (64
 independent rings of 2e3..2e5 particles in one persistent launch per stage,
@@ -496,22 +498,27 @@ def run_ours(args):
                "d2h_bytes_per_step": int(opos.nbytes + oalpha.nbytes),
                "wall_s": time.perf_counter() - t0}
 
+    # the one-GPU sub-lines (diagnostics, FP64, 64 rings, surrogate) and the
+    # CPU baseline run on rank 0 of a one-GPU run only: they do not change
+    # with N, and the other GPUs would be held idle meanwhile
+    extras = world == 1 and not args.no_extras
+    diag = None
     if rank == 0:
         ffma_peak, ffma2_peak = capi.fp32_peaks(local)
         fp32_peak = max(ffma_peak, ffma2_peak)
         rl = pair_roofline(pair_ms, pair_launches, pairs_timed, full_timed, fp32_peak)
-        diag = None if args.no_extras else run_diagnostics(ctx, stream, n, fp32_peak)
+        diag = run_diagnostics(ctx, stream, n, fp32_peak) if extras else None
     ctx.close()
     fp64 = unev = sur = None
-    if rank == 0 and not args.no_extras:
+    if rank == 0 and extras:
         fp64 = run_fp64(w, local, capi.fp64_peak(local))
         unev = run_uneven64(local, fp32_peak)
-    if rank == 0 and not args.no_surrogate:
+    if rank == 0 and world == 1 and not args.no_surrogate:
         sur = run_surrogate(args, local, shape)
 
     if rank == 0:
         traffic = NCU_TRAFFIC.get((n, shape[0], shape[1]))
-        cpu = cpu_baseline_leg(w)
+        cpu = cpu_baseline_leg(w) if world == 1 else None
         out = {
             "metric": "RK4 steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
