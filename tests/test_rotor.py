@@ -1,4 +1,4 @@
-"""The growing rotor wake at configuration 4's density: 4 tip vortices shedding
+"""The growing rotor wake at its full density: 4 tip vortices shedding
 200 particles per blade per step (10 deg per step, angular speed 10, so
 dt = pi/180), Gamma = 0.05, core 0.02, sigma = 0.03, inflow 0.05 applied after
 each RK3 step as PAWAN's operator split (wake.cpp:564-577).  Twenty steps on
@@ -52,7 +52,7 @@ def run_gpu(prec, split):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec,split", [(capi.FP64, False), (capi.FP32C, False), (capi.FP32C, True)])
-def test_rotor_wake_at_config4_density(gpu, reference, prec, split):
+def test_rotor_wake_at_full_density(gpu, reference, prec, split):
     x, a, v, da = run_gpu(prec, split)
     w = reference
     assert x.shape[0] == w.n == 4 * 200 * (STEPS + 1)

@@ -150,8 +150,8 @@ def test_octree_partitions_particles(gpu):
 
 @pytest.mark.parametrize("case", ["ring1m", "leapfrog1m"])
 def test_surrogate_vs_fp64_restatement(gpu, case):
-    """The quadrupole far field at 1M particles (the configuration-2 ring, and
-    two coaxial leapfrogging rings) against the oracle's FP64 restatement of
+    """The quadrupole far field at 1M particles (the 1000 x 1000 ring with
+    sigma = 0.02, and two coaxial leapfrogging rings) against the oracle's FP64 restatement of
     PAWAN's pair sum on 256 seeded targets: velocity and dalpha/dt both within
     the 1e-4 gate, with no fallback (so the surrogate's own result is what is
     compared)."""
