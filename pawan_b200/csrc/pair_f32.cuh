@@ -20,8 +20,9 @@
 // * In all-far tiles, positions are taken relative to the tile's first
 //   source, which turns the per-pair cross product alpha_s x d into per-source
 //   and per-group work (see the far loop): 25 packed FP32 operations per far
-//   pair.  In the other tiles cross products stay scalar, where a negated
-//   operand is free.
+//   pair.  In the other tiles the pair terms are packed too for shapes with
+//   two or more targets per thread (scalar for one target), and the cross
+//   products stay scalar, where a negated operand is free.
 #pragma once
 
 namespace pgpu {
@@ -261,6 +262,90 @@ __device__ __forceinline__ void pair_body_f32(const PairArgs<float> &a) {
               sd[k][1] = __ffma2_rn(fd, dy, sd[k][1]);
               sd[k][2] = __ffma2_rn(fd, dz, sd[k][2]);
             }
+          }
+        } else if constexpr (TPT >= 2) {
+          // Tiles with possible near pairs, shapes with two or more targets
+          // per thread: every pair takes the closed form, two sources per
+          // packed instruction (pair_terms_mid2: the mid formula, which beyond
+          // u = 50 equals the far limit to within e^{-u/2}); lanes at u < 1,
+          // the self pair among them, take the series.  Per pair: q (alpha_t x
+          // alpha_s) for the stretching (nearly parallel neighbours along a
+          // filament) and the diffusion v_t a_s - v_s a_t.  On the 1M ring
+          // this is 1% faster than the scalar path below at 128 x 2 and
+          // 256 x 2, and 2% slower at 256 x 1, which keeps the scalar path.
+          float2 sdv2[TPT][3];
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) sdv2[k][m] = make_float2(0.f, 0.f);
+          }
+#pragma unroll 1
+          for (int r = g; r < g + CG / 2; ++r) {
+            const float4 pa = sP[buf][2 * r], pb = sP[buf][2 * r + 1];
+            const float4 qa = sQ[buf][2 * r], qb = sQ[buf][2 * r + 1];
+            const float2 px = make_float2(pa.x, pa.y), py = make_float2(pa.z, pa.w), pz = make_float2(pb.x, pb.y);
+            const float2 ph = make_float2(pb.z, pb.w);
+            const float2 ax = make_float2(qa.x, qa.y), ay = make_float2(qa.z, qa.w), az = make_float2(qb.x, qb.y);
+            const float2 av = make_float2(qb.z, qb.w);
+            float2 lx = make_float2(0.f, 0.f), ly = lx, lz = lx;
+            if constexpr (SPLIT) {
+              const float4 la = sL[buf][2 * r], lb = sL[buf][2 * r + 1];
+              lx = make_float2(la.x, la.y); ly = make_float2(la.z, la.w); lz = make_float2(lb.x, lb.y);
+            }
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) {
+              float2 dx = __ffma2_rn(px, M1, X[k][0]);
+              float2 dy = __ffma2_rn(py, M1, X[k][1]);
+              float2 dz = __ffma2_rn(pz, M1, X[k][2]);
+              if constexpr (SPLIT) {
+                // the FP32 difference of nearby positions is exact; adding the
+                // difference of the residuals restores the FP64 difference
+                dx = __fadd2_rn(dx, __ffma2_rn(lx, M1, dup2(xl[k][0])));
+                dy = __fadd2_rn(dy, __ffma2_rn(ly, M1, dup2(xl[k][1])));
+                dz = __fadd2_rn(dz, __ffma2_rn(lz, M1, dup2(xl[k][2])));
+              }
+              float2 r2 = __fmul2_rn(dx, dx);
+              r2 = __ffma2_rn(dy, dy, r2);
+              r2 = __ffma2_rn(dz, dz, r2);
+              const float2 s2 = __fadd2_rn(dup2(hst[k]), ph);
+              PairTerms2 t = pair_terms_mid2(r2, s2);
+              const bool nx = r2.x < s2.x, ny = r2.y < s2.y;  // u < 1
+              if (__any_sync(0xffffffffu, nx || ny)) {
+                if (nx) { const PairTerms<float> e = pair_terms_near(r2.x, s2.x); t.q.x = e.q; t.F.x = e.F; t.zd.x = e.zd; }
+                if (ny) { const PairTerms<float> e = pair_terms_near(r2.y, s2.y); t.q.y = e.q; t.F.y = e.F; t.zd.y = e.zd; }
+              }
+              // pairs inside the far regime's bound count as full-formula pairs
+              nfull += (fmaf(-kFarU, ph.x, r2.x) < h50[k]) + (fmaf(-kFarU, ph.y, r2.y) < h50[k]);
+              // w = alpha_s x d (scalar: the negated operand is free)
+              const float2 wx = make_float2(ay.x * dz.x - az.x * dy.x, ay.y * dz.y - az.y * dy.y);
+              const float2 wy = make_float2(az.x * dx.x - ax.x * dz.x, az.y * dx.y - ax.y * dz.y);
+              const float2 wz = make_float2(ax.x * dy.x - ay.x * dx.x, ax.y * dy.y - ay.y * dx.y);
+              sv[k][0] = __ffma2_rn(t.q, wx, sv[k][0]);
+              sv[k][1] = __ffma2_rn(t.q, wy, sv[k][1]);
+              sv[k][2] = __ffma2_rn(t.q, wz, sv[k][2]);
+              float2 dot = __fmul2_rn(dup2(at[k][0]), wx);
+              dot = __ffma2_rn(dup2(at[k][1]), wy, dot);
+              dot = __ffma2_rn(dup2(at[k][2]), wz, dot);
+              const float2 fd = __fmul2_rn(t.F, dot);
+              sd[k][0] = __ffma2_rn(fd, dx, sd[k][0]);
+              sd[k][1] = __ffma2_rn(fd, dy, sd[k][1]);
+              sd[k][2] = __ffma2_rn(fd, dz, sd[k][2]);
+              const float2 cx = __ffma2_rn(dup2(at[k][1]), az, __fmul2_rn(dup2(-at[k][2]), ay));
+              const float2 cy = __ffma2_rn(dup2(at[k][2]), ax, __fmul2_rn(dup2(-at[k][0]), az));
+              const float2 cz = __ffma2_rn(dup2(at[k][0]), ay, __fmul2_rn(dup2(-at[k][1]), ax));
+              sp[k][0] = __ffma2_rn(t.q, cx, sp[k][0]);
+              sp[k][1] = __ffma2_rn(t.q, cy, sp[k][1]);
+              sp[k][2] = __ffma2_rn(t.q, cz, sp[k][2]);
+              const float2 VT = dup2(vt[k]);
+              sdv2[k][0] = __ffma2_rn(t.zd, __ffma2_rn(av, dup2(-at[k][0]), __fmul2_rn(VT, ax)), sdv2[k][0]);
+              sdv2[k][1] = __ffma2_rn(t.zd, __ffma2_rn(av, dup2(-at[k][1]), __fmul2_rn(VT, ay)), sdv2[k][1]);
+              sdv2[k][2] = __ffma2_rn(t.zd, __ffma2_rn(av, dup2(-at[k][2]), __fmul2_rn(VT, az)), sdv2[k][2]);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) sdv[k][m] += sdv2[k][m].x + sdv2[k][m].y;
           }
         } else {
           // Tiles with possible near pairs: scalar, one source at a time,
