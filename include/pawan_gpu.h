@@ -313,7 +313,9 @@ int pgpu_kernel_shapes(int *block, int *tpt, int max);
  *    "class": k, "nmin": .., "nmax": .., "block": .., "tpt": .., "ms": [one per shape]}
  * classes[i] (up to max_classes) describes the i-th class present, by
  * increasing size; *per_class = 1 if the classes launch separately.  The
- * rates of the current state are recomputed with the chosen launches. */
+ * rates of the current state are recomputed with the chosen launches.  A
+ * cache file that cannot be appended to gives PGPU_EINVAL after the choice
+ * is in place and the outputs are filled. */
 typedef struct pgpu_tune_class {
   int32_t size_class;        /* class index k */
   int32_t systems;           /* systems of the context in the class */

@@ -41,7 +41,7 @@ def needs_build() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
+    deps = [*CSRC.glob("*.cu"), *CSRC.glob("*.cuh"), *CSRC.glob("*.inc"), *(ROOT / "include").glob("*.h")]
     return any(p.stat().st_mtime > t for p in deps)
 
 

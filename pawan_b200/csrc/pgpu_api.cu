@@ -1282,6 +1282,9 @@ template <typename T> int time_subset(pgpu_ctx *c, const std::vector<int> &syste
   const int nch = choose_nch_for(c, shape, systems);
   std::vector<PlanEntry> plan = build_plan(c, systems, shape, nch);
   plan.resize(c->sys.size() + 1, plan.back());
+  // d_plan now holds this subset's plan: the next evaluation rebuilds the
+  // context's own, also when the tuning stops early on an error
+  c->plan_dirty = true;
   CK(cudaMemcpyAsync(c->d_plan, plan.data(), plan.size() * sizeof(PlanEntry), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   PairArgs<T> a;
@@ -1434,6 +1437,7 @@ int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tu
     c->sys_shape.clear();
     c->shape = single;
   }
+  bool cache_failed = false;
   if (cache_path && *cache_path) {
     if (FILE *f = fopen(cache_path, "a")) {
       for (size_t i = 0; i < K; ++i) {
@@ -1447,7 +1451,7 @@ int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tu
       }
       fclose(f);
     } else {
-      return fail(c, PGPU_EINVAL, "cannot append to the autotune cache %s", cache_path);
+      cache_failed = true;  // reported after the chosen launches are in place
     }
   }
   if (nclasses) *nclasses = (int)K;
@@ -1472,6 +1476,7 @@ int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tu
   if ((r = upload_plan(c))) return r;
   if ((r = pgpu_solve(c))) return r;
   pgpu_pair_kernel_time(c, nullptr, nullptr);
+  if (cache_failed) return fail(c, PGPU_EINVAL, "cannot append to the autotune cache %s", cache_path);
   return PGPU_OK;
 }
 
