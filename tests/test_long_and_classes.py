@@ -126,6 +126,28 @@ def test_autotune_classes_cache_round_trip(gpu, tmp_path):
     assert [(x["block"], x["tpt"]) for x in second["classes"]] == [(x["block"], x["tpt"]) for x in first["classes"]]
 
 
+@pytest.mark.gpu
+def test_autotune_classes_unwritable_cache_keeps_the_work_plan(gpu, tmp_path):
+    """A cache file that cannot be written is reported after the tuning has
+    put its choice in place: the context's rates afterwards are those of an
+    untuned context (the timing launches leave no plan or partials behind)."""
+    ws = cases.uneven_rings(count=12, nmin=2e3, nmax=6e4, seed=9)
+    assert len({capi_class(w.n) for w in ws}) >= 2
+    c, ids = batched(ws)
+    with pytest.raises(capi.PgpuError, match="cannot append to the autotune cache"):
+        c.autotune_classes(reps=1, cache=str(tmp_path / "no_such_dir" / "tune.jsonl"))
+    c.solve()
+    ref, rids = batched(ws)
+    ref.solve()
+    for i, r in zip(ids, rids):
+        v, a = c.rates(i)
+        vr, ar = ref.rates(r)
+        # other shapes and chunk counts only reorder the FP32 group sums
+        assert O.rel_err(v, vr) < 2e-6 and O.rel_err(a, ar) < 2e-6
+    c.close()
+    ref.close()
+
+
 def capi_class(n: int) -> int:
     k, hi = 0, 4096
     while n >= hi:
