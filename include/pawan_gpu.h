@@ -75,7 +75,8 @@ typedef struct pgpu_config {
 void pgpu_config_default(pgpu_config *cfg);
 
 /* Replaces: constructing a backend, `new pawan::__parallel(W)` (src/pawan.cpp:48,
- * src/interaction/parallel.cpp:11-12). */
+ * src/interaction/parallel.cpp:11-12).  On failure *ctx is NULL and
+ * pgpu_last_error(NULL) gives the reason (per calling thread). */
 int pgpu_create(pgpu_ctx **ctx, const pgpu_config *cfg);
 /* Replaces: the backend destructor (interaction.cpp:37-42). */
 int pgpu_destroy(pgpu_ctx *ctx);
@@ -455,8 +456,9 @@ int pgpu_fp64_peak(int device, double *tflops);
  * calls cudaMalloc or cudaFree: its intermediates live in one static device
  * array.  The first call on each device looks up that array's address and
  * clears its work counters (an asynchronous memset on `stream`, ordered
- * before that call's kernels), so make it before any stream capture.  Calls share the array: calls that overlap on the GPU (different
- * streams, or host threads without ordering) race and must not be issued.
+ * before that call's kernels), so make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU (different streams, or host
+ * threads without ordering) race and must not be issued.
  * n > PGPU_NOALLOC_MAX_N is rejected with PGPU_EINVAL; the reason is in
  * pgpu_noalloc_last_error(). */
 int pgpu_rates_noalloc(const double *pos, const double *alpha, const double *sigma, const double *vol, int64_t n,
@@ -464,6 +466,8 @@ int pgpu_rates_noalloc(const double *pos, const double *alpha, const double *sig
 /* Message for the last pgpu_rates_noalloc failure on the calling thread ("" after a success). */
 const char *pgpu_noalloc_last_error(void);
 
+/* Message of the last failure on ctx; with ctx NULL, of the calling thread's
+ * last pgpu_create ("" after a success). */
 const char *pgpu_last_error(pgpu_ctx *ctx);
 const char *pgpu_version(void);
 

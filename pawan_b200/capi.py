@@ -277,7 +277,7 @@ class Context:
         h = C.c_void_p()
         rc = self.lib.pgpu_create(C.byref(h), C.byref(cfg))
         if rc != PGPU_OK:
-            raise PgpuError(rc, "pgpu_create failed")
+            raise PgpuError(rc, self.lib.pgpu_last_error(None).decode())
         self.h = h
         self.wake_sizes: list[int] = []
         self.wake_system: list[int] = []

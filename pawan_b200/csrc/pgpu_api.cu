@@ -120,7 +120,7 @@ struct pgpu_ctx {
   bool plan_dirty = true;
   bool timing = true;
   bool capturing = false;
-  cudaEvent_t ev[8][2];
+  cudaEvent_t ev[8][2] = {};
   double pair_ms = 0.0;
   int64_t pair_launches = 0;
   int64_t launches = 0;
@@ -176,6 +176,26 @@ int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
       return fail(c, PGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_));                   \
     }                                                                                               \
   } while (0)
+
+// Why the calling thread's last pgpu_create failed ("" after a success);
+// pgpu_last_error(NULL) returns it.
+thread_local char g_create_err[512] = "";
+
+// Releases what pgpu_create made before it failed, and records why.
+int create_fail(pgpu_ctx *c, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_create_err, sizeof(g_create_err), fmt, ap);
+  va_end(ap);
+  if (c) {
+    for (auto &pair : c->ev)
+      for (cudaEvent_t e : pair)
+        if (e) cudaEventDestroy(e);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+  }
+  return code;
+}
 
 bool fp64(const pgpu_ctx *c) { return c->cfg.precision == PGPU_FP64; }
 // The FP32C Gaussian pair kernel tests whole source tiles against boxes
@@ -594,18 +614,31 @@ void pgpu_config_default(pgpu_config *cfg) {
 const char *pgpu_version(void) { return "pawan_b200 0.1 (sm_100a)"; }
 
 int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
-  if (!out) return PGPU_EINVAL;
+  if (!out) return create_fail(nullptr, PGPU_EINVAL, "no output pointer for the context");
   *out = nullptr;
   pgpu_ctx *c = new pgpu_ctx;
   if (cfg) c->cfg = *cfg;
   else pgpu_config_default(&c->cfg);
-  if (c->cfg.precision != PGPU_FP32C && c->cfg.precision != PGPU_FP64) {
-    delete c;
-    return PGPU_EINVAL;
-  }
-  if (c->cfg.kernel != PGPU_KERNEL_GAUSSIAN && c->cfg.kernel != PGPU_KERNEL_HIGHORDER) {
-    delete c;
-    return PGPU_EINVAL;
+  if (c->cfg.precision != PGPU_FP32C && c->cfg.precision != PGPU_FP64)
+    return create_fail(c, PGPU_EINVAL, "unknown precision %d", c->cfg.precision);
+  if (c->cfg.kernel != PGPU_KERNEL_GAUSSIAN && c->cfg.kernel != PGPU_KERNEL_HIGHORDER)
+    return create_fail(c, PGPU_EINVAL, "unknown regularisation kernel %d", c->cfg.kernel);
+  if (c->cfg.block > 0 || c->cfg.tpt > 0) {
+    int found = -1;
+    for (int s = 0; s < kNumShapes; ++s)
+      if ((c->cfg.block <= 0 || kShapes[s].block == c->cfg.block) && (c->cfg.tpt <= 0 || kShapes[s].tpt == c->cfg.tpt)) {
+        found = s;
+        break;
+      }
+    if (found < 0)
+      return create_fail(c, PGPU_EINVAL, "no compiled pair-kernel shape with block %d and %d targets per thread",
+                         c->cfg.block, c->cfg.tpt);
+    c->shape = found;
+  } else if (c->cfg.kernel == PGPU_KERNEL_GAUSSIAN) {
+    // untuned defaults: the fastest Gaussian shapes on the 1M ring, FP32C
+    // 128 x 2 (1075 ms per evaluation against 1163 ms for 256 x 1) and FP64
+    // 128 x 1 (3.09 s against 3.22 s)
+    c->shape = c->cfg.precision == PGPU_FP32C ? 1 : 0;
   }
   cudaError_t e = cudaSetDevice(c->cfg.device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
@@ -615,28 +648,10 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev[k][1]);
   }
   if (e != cudaSuccess) {
-    delete c;
-    return PGPU_ECUDA;
+    cudaGetLastError();
+    return create_fail(c, PGPU_ECUDA, "device %d: %s", c->cfg.device, cudaGetErrorString(e));
   }
-  if (c->cfg.block > 0 || c->cfg.tpt > 0) {
-    int found = -1;
-    for (int s = 0; s < kNumShapes; ++s)
-      if ((c->cfg.block <= 0 || kShapes[s].block == c->cfg.block) && (c->cfg.tpt <= 0 || kShapes[s].tpt == c->cfg.tpt)) {
-        found = s;
-        break;
-      }
-    if (found < 0) {
-      cudaStreamDestroy(c->st);
-      delete c;
-      return PGPU_EINVAL;
-    }
-    c->shape = found;
-  } else if (c->cfg.kernel == PGPU_KERNEL_GAUSSIAN) {
-    // untuned defaults: the fastest Gaussian shapes on the 1M ring, FP32C
-    // 128 x 2 (1075 ms per evaluation against 1163 ms for 256 x 1) and FP64
-    // 128 x 1 (3.09 s against 3.22 s)
-    c->shape = c->cfg.precision == PGPU_FP32C ? 1 : 0;
-  }
+  g_create_err[0] = '\0';
   *out = c;
   return PGPU_OK;
 }
@@ -1563,7 +1578,7 @@ int pgpu_fp32_peak(int device, double *tflops, double *ms_out) {
   return PGPU_OK;
 }
 
-const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err : "null context"; }
+const char *pgpu_last_error(pgpu_ctx *c) { return c ? c->err : g_create_err; }
 
 }  // extern "C"
 

@@ -32,7 +32,7 @@ __gpu::~__gpu() {
 void __gpu::check(int rc) const {
   if (rc != PGPU_OK) {
     std::string msg = "pawan_gpu: ";
-    msg += _ctx ? pgpu_last_error(_ctx) : "context creation failed";
+    msg += pgpu_last_error(_ctx);  // with no context yet: why pgpu_create failed
     throw std::runtime_error(msg + " (status " + std::to_string(rc) + ")");
   }
 }

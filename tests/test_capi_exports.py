@@ -33,3 +33,16 @@ def test_version_and_shapes_without_gpu():
     assert b"sm_100a" in lib.pgpu_version()
     shapes = capi.kernel_shapes()
     assert (256, 2) in shapes and len(shapes) >= 4
+
+
+@pytest.mark.parametrize("kw, msg", [({"precision": 7}, "unknown precision 7"),
+                                     ({"kernel": 5}, "unknown regularisation kernel 5"),
+                                     ({"block": 96}, "no compiled pair-kernel shape with block 96")])
+def test_invalid_config_is_rejected_before_any_device_call(kw, msg):
+    # the configuration is checked before pgpu_create touches a device, so
+    # this runs without a GPU; the reason comes back through
+    # pgpu_last_error(NULL)
+    capi.load(build_if_missing=True)
+    with pytest.raises(capi.PgpuError, match=msg) as e:
+        capi.Context(**kw)
+    assert e.value.code == capi.PGPU_EINVAL
