@@ -18,6 +18,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -150,6 +151,37 @@ namespace {
 struct NvtxRange {
   explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
   ~NvtxRange() { nvtxRangePop(); }
+};
+
+// Makes a context's (or network's) device current for one entry point and
+// restores the caller's device on return, so that contexts on different GPUs
+// can be driven from one host thread.  With the device already current (the
+// one-GPU case) it calls nothing but cudaGetDevice.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope &) = delete;
+  DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
+// Restores the caller's current device on return, for the calls that select
+// a device themselves (and check that it exists).
+struct RestoreDevice {
+  int prev = -1;
+  RestoreDevice() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~RestoreDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  RestoreDevice(const RestoreDevice &) = delete;
+  RestoreDevice &operator=(const RestoreDevice &) = delete;
 };
 
 int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
@@ -640,6 +672,7 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
     // 128 x 1 (3.09 s against 3.22 s)
     c->shape = c->cfg.precision == PGPU_FP32C ? 1 : 0;
   }
+  RestoreDevice restore_device;
   cudaError_t e = cudaSetDevice(c->cfg.device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device);
@@ -658,6 +691,7 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
 
 int pgpu_destroy(pgpu_ctx *c) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   cudaStreamSynchronize(c->st);
   surrogate_free(c);
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
@@ -683,6 +717,7 @@ int pgpu_destroy(pgpu_ctx *c) {
 
 int pgpu_add_wake(pgpu_ctx *c, int32_t system, int64_t capacity, int32_t *wake_id) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (c->frozen) return fail(c, PGPU_EINVAL, "wakes must be added before the first particle upload");
   if (system < 0 || system > 1 << 20) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   if (capacity < 0 || capacity > (int64_t)1 << 31) return fail(c, PGPU_EINVAL, "invalid capacity %lld", (long long)capacity);
@@ -698,6 +733,7 @@ int pgpu_set_particles(pgpu_ctx *c, int32_t wake, int64_t n, const double *pos, 
                        const double *sigma, const double *vol) {
   int r = wake_ok(c, wake);
   if (r) return r;
+  DeviceScope device_scope(c->cfg.device);
   if ((r = freeze(c))) return r;
   WakeRec &W = c->wakes[wake];
   if (n < 0 || n > W.cap) return fail(c, PGPU_EINVAL, "n=%lld exceeds the capacity %lld of wake %d", (long long)n, (long long)W.cap, wake);
@@ -711,6 +747,7 @@ int pgpu_append_particles(pgpu_ctx *c, int32_t wake, int64_t m, const double *po
                           const double *sigma, const double *vol) {
   int r = wake_ok(c, wake);
   if (r) return r;
+  DeviceScope device_scope(c->cfg.device);
   if ((r = freeze(c))) return r;
   WakeRec &W = c->wakes[wake];
   if (c->sys[W.sys].wakes.back() != wake) return fail(c, PGPU_EINVAL, "only the last wake of a system can grow");
@@ -744,6 +781,7 @@ static int download_rows(pgpu_ctx *c, const double *src, const WakeRec &W, doubl
 int pgpu_get_state(pgpu_ctx *c, int32_t wake, double *pos, double *alpha) {
   int r = wake_ok(c, wake);
   if (r) return r;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (!pos || !alpha) return fail(c, PGPU_EINVAL, "null output array");
   return download_rows(c, c->x0, c->wakes[wake], pos, alpha);
@@ -752,6 +790,7 @@ int pgpu_get_state(pgpu_ctx *c, int32_t wake, double *pos, double *alpha) {
 int pgpu_get_rates(pgpu_ctx *c, int32_t wake, double *vel, double *dalpha) {
   int r = wake_ok(c, wake);
   if (r) return r;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (!vel || !dalpha) return fail(c, PGPU_EINVAL, "null output array");
   return download_rows(c, c->rates, c->wakes[wake], vel, dalpha);
@@ -759,6 +798,7 @@ int pgpu_get_rates(pgpu_ctx *c, int32_t wake, double *vel, double *dalpha) {
 
 static int flat_io(pgpu_ctx *c, double *flat, const int64_t *maxn, int32_t nwakes, int dir, const double *soa_src) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (!flat || !maxn || nwakes != (int32_t)c->wakes.size()) return fail(c, PGPU_EINVAL, "flat state needs one capacity per wake");
   int64_t off = 0;
@@ -804,6 +844,7 @@ int pgpu_get_rates_flat(pgpu_ctx *c, double *rate, const int64_t *maxn, int32_t 
 int pgpu_solve(pgpu_ctx *c) {
   NvtxRange nvtx("pgpu_solve");
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   int r = upload_plan(c);
   if (r) return r;
@@ -814,6 +855,7 @@ int pgpu_solve(pgpu_ctx *c) {
 
 int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t count) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   if (uses_split(c) && count >= 0)
     return fail(c, PGPU_EINVAL, "split positions are not exchanged between contexts: use one context per system");
@@ -830,6 +872,7 @@ int pgpu_set_target_range(pgpu_ctx *c, int32_t system, int64_t first, int64_t co
 int pgpu_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
   NvtxRange nvtx("pgpu_stage");
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
   if (stage < 0 || stage >= stages_of(scheme)) return fail(c, PGPU_EINVAL, "stage %d out of range for scheme %d", stage, scheme);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
@@ -842,6 +885,7 @@ int pgpu_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
 
 int pgpu_records(pgpu_ctx *c, int32_t system, void **P, void **Q) {
   if (!c || !P || !Q) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   const size_t rb = rec_bytes(c);
@@ -853,6 +897,7 @@ int pgpu_records(pgpu_ctx *c, int32_t system, void **P, void **Q) {
 int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
   NvtxRange nvtx("pgpu_step");
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (scheme != PGPU_EULER && scheme != PGPU_RK3 && scheme != PGPU_RK4) return fail(c, PGPU_EINVAL, "unknown scheme %d", scheme);
   if (nsteps < 0) return fail(c, PGPU_EINVAL, "negative step count");
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
@@ -899,6 +944,7 @@ int pgpu_step(pgpu_ctx *c, int scheme, double dt, int32_t nsteps) {
 int pgpu_diagnose_partial(pgpu_ctx *c, int32_t system, double *fields) {
   NvtxRange nvtx("pgpu_diagnose_partial");
   if (!c || !fields) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   int r = check_contiguous(c);
@@ -987,6 +1033,7 @@ int pgpu_diagnose_combine(const double *fields, int32_t nwakes, double zc_prev, 
 int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
   NvtxRange nvtx("pgpu_diagnose");
   if (!c || !out) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (restricted(c))
     return fail(c, PGPU_EINVAL, "with target ranges each context holds a part of the diagnostics: sum "
@@ -1003,6 +1050,7 @@ int pgpu_diagnose(pgpu_ctx *c, int32_t system, double *out, double *vbi) {
 
 int pgpu_probe(pgpu_ctx *c, int32_t system, int64_t npts, const double *pts, double *vel) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   if (npts < 0 || (npts > 0 && (!pts || !vel))) return fail(c, PGPU_EINVAL, "bad probe arrays");
@@ -1026,6 +1074,7 @@ int pgpu_probe(pgpu_ctx *c, int32_t system, int64_t npts, const double *pts, dou
 
 int pgpu_sync(pgpu_ctx *c) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   CK(cudaStreamSynchronize(c->st));
   if (c->frozen) {
     int flag = 0;
@@ -1040,6 +1089,7 @@ int pgpu_sync(pgpu_ctx *c) {
 
 int pgpu_influence(pgpu_ctx *c) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   NvtxRange nvtx("pgpu_influence");
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   int r = check_contiguous(c);
@@ -1084,6 +1134,7 @@ int pgpu_influence(pgpu_ctx *c) {
 int pgpu_get_vorticity_field(pgpu_ctx *c, int32_t wake, double *field) {
   int r = wake_ok(c, wake);
   if (r) return r;
+  DeviceScope device_scope(c->cfg.device);
   if (!field) return fail(c, PGPU_EINVAL, "null output array");
   if (!c->d_field) return fail(c, PGPU_EINVAL, "no vorticity field was computed (pgpu_influence)");
   const WakeRec &W = c->wakes[wake];
@@ -1093,12 +1144,14 @@ int pgpu_get_vorticity_field(pgpu_ctx *c, int32_t wake, double *field) {
 
 int pgpu_set_timing(pgpu_ctx *c, int on) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   c->timing = on != 0;
   return PGPU_OK;
 }
 
 int pgpu_sync_timeout(pgpu_ctx *c, double seconds) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   NvtxRange nvtx("pgpu_sync_timeout");
   const auto t0 = std::chrono::steady_clock::now();
   for (;;) {
@@ -1116,6 +1169,7 @@ int pgpu_sync_timeout(pgpu_ctx *c, double seconds) {
 int pgpu_snapshot_begin(pgpu_ctx *c, int32_t slot) {
   NvtxRange nvtx("pgpu_snapshot_begin");
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (slot != 0 && slot != 1) return fail(c, PGPU_EINVAL, "snapshot slot %d is not 0 or 1", slot);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (c->capturing) return fail(c, PGPU_EINVAL, "a snapshot cannot be taken during graph capture");
@@ -1172,6 +1226,7 @@ int pgpu_snapshot_wait(pgpu_ctx *c, int32_t slot, double seconds, const double *
                        int32_t nwakes) {
   NvtxRange nvtx("pgpu_snapshot_wait");
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (slot != 0 && slot != 1) return fail(c, PGPU_EINVAL, "snapshot slot %d is not 0 or 1", slot);
   if (!c->snap_begun[slot]) return fail(c, PGPU_EINVAL, "no snapshot was begun in slot %d", slot);
   if (seconds > 0) {
@@ -1199,6 +1254,7 @@ int pgpu_snapshot_wait(pgpu_ctx *c, int32_t slot, double seconds, const double *
 
 int pgpu_pair_kernel_time(pgpu_ctx *c, double *ms, int64_t *launches) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (ms) *ms = c->pair_ms;
   if (launches) *launches = c->pair_launches;
   c->pair_ms = 0.0;
@@ -1210,6 +1266,7 @@ int64_t pgpu_launch_count(pgpu_ctx *c) { return c ? c->launches : -1; }
 
 int pgpu_pair_counts(pgpu_ctx *c, int64_t *pairs, int64_t *full_pairs) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   int64_t full = c->pairs_acc;
   // the Gaussian kernel has a far regime in both precisions (and counts its
   // full-formula pairs); the high-order kernel evaluates every pair in full
@@ -1237,6 +1294,7 @@ int pgpu_kernel_shapes(int *block, int *tpt, int max) {
 
 int pgpu_autotune(pgpu_ctx *c, int reps, int *block, int *tpt, double *ms_per_launch) {
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (reps < 1) reps = 1;
   c->sys_shape.clear();  // one shape for every system from here on
@@ -1374,6 +1432,7 @@ int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tu
                           int *nclasses, int *per_class) {
   NvtxRange nvtx("pgpu_autotune_classes");
   if (!c) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (c->sur) return fail(c, PGPU_EINVAL, "the surrogate evaluates one system; use pgpu_autotune");
   if (reps < 1) reps = 1;
@@ -1497,12 +1556,14 @@ int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tu
 
 int pgpu_get_stream(pgpu_ctx *c, void **stream) {
   if (!c || !stream) return PGPU_EINVAL;
+  DeviceScope device_scope(c->cfg.device);
   *stream = (void *)c->st;
   return PGPU_OK;
 }
 
 int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops) {
   pgpu_ctx *c = nullptr;  // for CK's error path
+  RestoreDevice restore_device;
   CK(cudaSetDevice(device));
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -1541,6 +1602,7 @@ int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops) {
 
 int pgpu_fp64_peak(int device, double *tflops) {
   pgpu_ctx *c = nullptr;  // for CK's error path
+  RestoreDevice restore_device;
   CK(cudaSetDevice(device));
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
