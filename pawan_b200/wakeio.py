@@ -74,7 +74,17 @@ def read_diagnosis(path) -> tuple[float, np.ndarray]:
 
 
 def write_wake_record(f, t: float, wakes: list[WakeRecord], maxn: int) -> None:
-    """Appends one .wake record (the high 4 bytes of the maxN field are written as 0)."""
+    """Appends one .wake record (the high 4 bytes of the maxN field are written as 0).
+    Every wake holds all maxN capacity rows, as PAWAN writes them; arrays of
+    another length are rejected before anything is written."""
+    for k, w in enumerate(wakes):
+        shapes = {"pos": (maxn, 3), "alpha": (maxn, 3), "radius": (maxn,), "active": (maxn,), "volume": (maxn,),
+                  "birth": (maxn,)}
+        for name, shape in shapes.items():
+            if np.shape(getattr(w, name)) != shape:
+                raise ValueError(f"wake {k}: {name} has shape {np.shape(getattr(w, name))}, expected {shape}")
+        if not 0 <= w.n <= maxn:
+            raise ValueError(f"wake {k}: {w.n} particles do not fit {maxn} rows")
     f.write(struct.pack("<dQiI", t, len(wakes), maxn, 0))
     for w in wakes:
         f.write(struct.pack("<Q", w.n))

@@ -71,6 +71,24 @@ def test_writer_roundtrip(tmp_path):
     assert raw0 == raw1
 
 
+def test_writer_rejects_rows_short_of_capacity(tmp_path):
+    # PAWAN writes every capacity row of a wake; a record with fewer rows
+    # would shift every later field of the file
+    (t, ws), = wakeio.read_wake(GOLD / "integrate" / "ring1000_rk4.wake")[:1]
+    maxn = ws[0].pos.shape[0]
+    short = wakeio.WakeRecord(ws[0].n, ws[0].pos[:-1], ws[0].alpha, ws[0].radius, ws[0].active, ws[0].volume,
+                              ws[0].birth)
+    p = tmp_path / "short.wake"
+    with open(p, "wb") as f:
+        with pytest.raises(ValueError, match="pos has shape"):
+            wakeio.write_wake_record(f, t, [short], maxn)
+        too_many = wakeio.WakeRecord(maxn + 1, *[getattr(ws[0], k) for k in
+                                                 ("pos", "alpha", "radius", "active", "volume", "birth")])
+        with pytest.raises(ValueError, match="do not fit"):
+            wakeio.write_wake_record(f, t, [too_many], maxn)
+    assert p.stat().st_size == 0
+
+
 def test_driver_reference_mode_reproduces_golden(driver, tmp_path, ref_available):
     g = np.load(GOLD / "ring1000.npz")
     w = cases.Wake(g["pos"], g["alpha"], g["sigma"], g["vol"])
