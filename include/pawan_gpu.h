@@ -11,10 +11,11 @@
  * and strengths are row-major (n, 3) FP64 host arrays, radii and volumes (n).
  *
  * A context owns all device memory and one CUDA stream; it is used from one
- * host thread at a time (PAWAN calls its solver from one thread).  Each call
- * on a context (or network) works on that object's device and leaves the
- * caller's current device as it found it, so contexts on several GPUs can be
- * driven from one thread.  Wakes are
+ * host thread at a time (PAWAN calls its solver from one thread).
+ * pgpu_create (and pgpu_mlp_create) make the new object's device current, as
+ * cudaSetDevice does; every later call that works on the device makes that
+ * object's device current for its duration and then restores the caller's, so
+ * contexts on several GPUs can be driven from one thread.  Wakes are
  * grouped into systems: the wakes of one system all interact with one another,
  * exactly as the wakes held by one PAWAN __interaction do
  * (src/interaction/interaction.cpp:196-210); different systems are independent

@@ -153,10 +153,13 @@ struct NvtxRange {
   ~NvtxRange() { nvtxRangePop(); }
 };
 
-// Makes a context's (or network's) device current for one entry point and
-// restores the caller's device on return, so that contexts on different GPUs
-// can be driven from one host thread.  With the device already current (the
-// one-GPU case) it calls nothing but cudaGetDevice.
+// Makes a context's (or network's) device current for one entry point that
+// works on the device, and restores the caller's device on return, so that
+// contexts on different GPUs can be driven from one host thread.  pgpu_create
+// leaves the new context's device current (as cudaSetDevice would), so a
+// thread that creates a context and then uses it never switches: it calls
+// nothing but cudaGetDevice.  Host-only calls and pgpu_snapshot_wait (which
+// writer threads call; events need no current device) do not switch.
 struct DeviceScope {
   int prev = -1;
   explicit DeviceScope(int dev) {
@@ -168,20 +171,6 @@ struct DeviceScope {
   }
   DeviceScope(const DeviceScope &) = delete;
   DeviceScope &operator=(const DeviceScope &) = delete;
-};
-
-// Restores the caller's current device on return, for the calls that select
-// a device themselves (and check that it exists).
-struct RestoreDevice {
-  int prev = -1;
-  RestoreDevice() {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-  }
-  ~RestoreDevice() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-  RestoreDevice(const RestoreDevice &) = delete;
-  RestoreDevice &operator=(const RestoreDevice &) = delete;
 };
 
 int fail(pgpu_ctx *c, int code, const char *fmt, ...) {
@@ -672,7 +661,6 @@ int pgpu_create(pgpu_ctx **out, const pgpu_config *cfg) {
     // 128 x 1 (3.09 s against 3.22 s)
     c->shape = c->cfg.precision == PGPU_FP32C ? 1 : 0;
   }
-  RestoreDevice restore_device;
   cudaError_t e = cudaSetDevice(c->cfg.device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device);
@@ -717,7 +705,6 @@ int pgpu_destroy(pgpu_ctx *c) {
 
 int pgpu_add_wake(pgpu_ctx *c, int32_t system, int64_t capacity, int32_t *wake_id) {
   if (!c) return PGPU_EINVAL;
-  DeviceScope device_scope(c->cfg.device);
   if (c->frozen) return fail(c, PGPU_EINVAL, "wakes must be added before the first particle upload");
   if (system < 0 || system > 1 << 20) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   if (capacity < 0 || capacity > (int64_t)1 << 31) return fail(c, PGPU_EINVAL, "invalid capacity %lld", (long long)capacity);
@@ -885,7 +872,6 @@ int pgpu_stage(pgpu_ctx *c, int scheme, int stage, double dt) {
 
 int pgpu_records(pgpu_ctx *c, int32_t system, void **P, void **Q) {
   if (!c || !P || !Q) return PGPU_EINVAL;
-  DeviceScope device_scope(c->cfg.device);
   if (!c->frozen) return fail(c, PGPU_EINVAL, "no particles were uploaded");
   if (system < 0 || system >= (int32_t)c->sys.size()) return fail(c, PGPU_EINVAL, "invalid system id %d", system);
   const size_t rb = rec_bytes(c);
@@ -1144,7 +1130,6 @@ int pgpu_get_vorticity_field(pgpu_ctx *c, int32_t wake, double *field) {
 
 int pgpu_set_timing(pgpu_ctx *c, int on) {
   if (!c) return PGPU_EINVAL;
-  DeviceScope device_scope(c->cfg.device);
   c->timing = on != 0;
   return PGPU_OK;
 }
@@ -1226,7 +1211,6 @@ int pgpu_snapshot_wait(pgpu_ctx *c, int32_t slot, double seconds, const double *
                        int32_t nwakes) {
   NvtxRange nvtx("pgpu_snapshot_wait");
   if (!c) return PGPU_EINVAL;
-  DeviceScope device_scope(c->cfg.device);
   if (slot != 0 && slot != 1) return fail(c, PGPU_EINVAL, "snapshot slot %d is not 0 or 1", slot);
   if (!c->snap_begun[slot]) return fail(c, PGPU_EINVAL, "no snapshot was begun in slot %d", slot);
   if (seconds > 0) {
@@ -1254,7 +1238,6 @@ int pgpu_snapshot_wait(pgpu_ctx *c, int32_t slot, double seconds, const double *
 
 int pgpu_pair_kernel_time(pgpu_ctx *c, double *ms, int64_t *launches) {
   if (!c) return PGPU_EINVAL;
-  DeviceScope device_scope(c->cfg.device);
   if (ms) *ms = c->pair_ms;
   if (launches) *launches = c->pair_launches;
   c->pair_ms = 0.0;
@@ -1556,14 +1539,12 @@ int pgpu_autotune_classes(pgpu_ctx *c, int reps, const char *cache_path, pgpu_tu
 
 int pgpu_get_stream(pgpu_ctx *c, void **stream) {
   if (!c || !stream) return PGPU_EINVAL;
-  DeviceScope device_scope(c->cfg.device);
   *stream = (void *)c->st;
   return PGPU_OK;
 }
 
 int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops) {
   pgpu_ctx *c = nullptr;  // for CK's error path
-  RestoreDevice restore_device;
   CK(cudaSetDevice(device));
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -1602,7 +1583,6 @@ int pgpu_fp32_peaks(int device, double *ffma_tflops, double *ffma2_tflops) {
 
 int pgpu_fp64_peak(int device, double *tflops) {
   pgpu_ctx *c = nullptr;  // for CK's error path
-  RestoreDevice restore_device;
   CK(cudaSetDevice(device));
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
