@@ -248,6 +248,20 @@ def rates_noalloc(pos: int, alpha: int, sigma: int, vol: int, n: int, nu: float,
         raise PgpuError(rc, lib.pgpu_noalloc_last_error().decode())
 
 
+def wake_arrays(w) -> list[np.ndarray]:
+    """Contiguous FP64 (pos, alpha, sigma, vol) of a wake of w.n particles.
+    The library reads the first 3n, 3n, n and n values of them (row-major), so
+    shorter arrays are rejected here instead of being over-read."""
+    n = int(w.n)
+    out = []
+    for name, per in (("pos", 3), ("alpha", 3), ("sigma", 1), ("vol", 1)):
+        a = _c(getattr(w, name))
+        if a.size < per * n:
+            raise ValueError(f"{name} holds {a.size} values; a wake of {n} particles needs {per * n}")
+        out.append(a)
+    return out
+
+
 def kernel_shapes() -> list[tuple[int, int]]:
     lib = load()
     b = (C.c_int * 32)()
@@ -312,12 +326,12 @@ class Context:
         return wid.value
 
     def set_particles(self, wake: int, w):
-        arr = [_c(w.pos), _c(w.alpha), _c(w.sigma), _c(w.vol)]
+        arr = wake_arrays(w)
         self._ck(self.lib.pgpu_set_particles(self.h, wake, w.n, *[_p(a) for a in arr]))
         self.wake_sizes[wake] = w.n
 
     def append_particles(self, wake: int, w):
-        arr = [_c(w.pos), _c(w.alpha), _c(w.sigma), _c(w.vol)]
+        arr = wake_arrays(w)
         self._ck(self.lib.pgpu_append_particles(self.h, wake, w.n, *[_p(a) for a in arr]))
         self.wake_sizes[wake] += w.n
 
@@ -330,6 +344,10 @@ class Context:
         n = self.num_particles(wake)
         if out is None:
             out = (np.zeros((n, 3)), np.zeros((n, 3)))
+        for a in out:
+            # written in place: contiguous FP64 with room for the wake's n rows
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.size >= 3 * n):
+                raise ValueError(f"state output arrays must be C-contiguous float64 with room for {3 * n} values")
         self._ck(self.lib.pgpu_get_state(self.h, wake, _p(out[0]), _p(out[1])))
         return out
 

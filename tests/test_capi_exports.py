@@ -46,3 +46,22 @@ def test_invalid_config_is_rejected_before_any_device_call(kw, msg):
     with pytest.raises(capi.PgpuError, match=msg) as e:
         capi.Context(**kw)
     assert e.value.code == capi.PGPU_EINVAL
+
+
+def test_wake_arrays_reject_short_arrays():
+    # the library reads 3n, 3n, n and n values: a short array would be
+    # over-read on the host, so the binding refuses it before any call
+    import numpy as np
+
+    from pawan_b200 import cases
+    w = cases.ring_stations(stations=8, seed=0)
+    arr = capi.wake_arrays(w)
+    assert [a.size for a in arr] == [3 * w.n, 3 * w.n, w.n, w.n]
+    assert all(a.dtype == np.float64 and a.flags.c_contiguous for a in arr)
+    # contiguous FP64 input is passed through without a copy
+    assert arr[0] is w.pos or np.shares_memory(arr[0], w.pos)
+    short = cases.Wake(w.pos, w.alpha, w.sigma[:-1], w.vol)
+    with pytest.raises(ValueError, match="sigma holds"):
+        capi.wake_arrays(short)
+    with pytest.raises(ValueError, match="alpha holds"):
+        capi.wake_arrays(cases.Wake(w.pos, w.alpha[:-1], w.sigma, w.vol))
