@@ -248,6 +248,21 @@ def rates_noalloc(pos: int, alpha: int, sigma: int, vol: int, n: int, nu: float,
         raise PgpuError(rc, lib.pgpu_noalloc_last_error().decode())
 
 
+def surrogate_config(**kw) -> SurrogateConfig:
+    """pgpu_surrogate_config_default with the given fields replaced; an
+    unknown field name is an error (a ctypes structure would otherwise keep
+    it as a plain attribute that the library never sees)."""
+    lib = load()
+    cfg = SurrogateConfig()
+    lib.pgpu_surrogate_config_default(C.byref(cfg))
+    fields = {name for name, _ in SurrogateConfig._fields_}
+    for k, v in kw.items():
+        if k not in fields:
+            raise TypeError(f"unknown surrogate setting {k!r} (fields: {', '.join(sorted(fields))})")
+        setattr(cfg, k, v)
+    return cfg
+
+
 def wake_arrays(w) -> list[np.ndarray]:
     """Contiguous FP64 (pos, alpha, sigma, vol) of a wake of w.n particles.
     The library reads the first 3n, 3n, n and n values of them (row-major), so
@@ -478,10 +493,7 @@ class Context:
         return P.value, Q.value
 
     def surrogate_enable(self, system: int = 0, **kw):
-        cfg = SurrogateConfig()
-        self.lib.pgpu_surrogate_config_default(C.byref(cfg))
-        for k, v in kw.items():
-            setattr(cfg, k, v)
+        cfg = surrogate_config(**kw)
         self._ck(self.lib.pgpu_surrogate_enable(self.h, system, C.byref(cfg)))
 
     def surrogate_disable(self):

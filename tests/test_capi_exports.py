@@ -65,3 +65,12 @@ def test_wake_arrays_reject_short_arrays():
         capi.wake_arrays(short)
     with pytest.raises(ValueError, match="alpha holds"):
         capi.wake_arrays(cases.Wake(w.pos, w.alpha[:-1], w.sigma, w.vol))
+
+
+def test_surrogate_config_defaults_and_unknown_settings():
+    # pgpu_surrogate_config_default is host-only: no GPU needed
+    cfg = capi.surrogate_config(order=3, near_widths=4.5)
+    assert cfg.order == 3 and cfg.near_widths == 4.5
+    assert cfg.tolerance == 1e-4 and cfg.leaf_size == 256 and cfg.check_targets == 4096
+    with pytest.raises(TypeError, match="unknown surrogate setting 'near_width'"):
+        capi.surrogate_config(near_width=4.0)
