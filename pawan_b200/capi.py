@@ -575,6 +575,18 @@ def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+MLP_IN, MLP_OUT = 24, 6  # features per row in, outputs per row out
+
+
+def _rows(a, cols: int, name: str) -> np.ndarray:
+    """Contiguous FP32 (rows, cols) view of a; any other shape is an error,
+    since the library reads rows x cols values."""
+    a = _f32(a)
+    if a.ndim != 2 or a.shape[1] != cols:
+        raise ValueError(f"{name} must have shape (rows, {cols}), not {a.shape}")
+    return a
+
+
 class Mlp:
     """The far-field correction network (see include/pawan_gpu.h)."""
 
@@ -611,23 +623,26 @@ class Mlp:
     @params.setter
     def params(self, p):
         p = _f32(p)
-        assert p.shape == (self.n_params,)
+        if p.shape != (self.n_params,):
+            raise ValueError(f"params must have shape ({self.n_params},), not {p.shape}")
         self._ck(self.lib.pgpu_mlp_set_params(self.h, p.ctypes.data_as(_fp)))
 
     def forward(self, x) -> np.ndarray:
-        x = _f32(x)
-        y = np.zeros((x.shape[0], 6), np.float32)
+        x = _rows(x, MLP_IN, "x")
+        y = np.zeros((x.shape[0], MLP_OUT), np.float32)
         self._ck(self.lib.pgpu_mlp_forward(self.h, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)))
         return y
 
     def forward_fused(self, x) -> np.ndarray:
-        x = _f32(x)
-        y = np.zeros((x.shape[0], 6), np.float32)
+        x = _rows(x, MLP_IN, "x")
+        y = np.zeros((x.shape[0], MLP_OUT), np.float32)
         self._ck(self.lib.pgpu_mlp_forward_fused(self.h, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)))
         return y
 
     def gradient(self, x, t):
-        x, t = _f32(x), _f32(t)
+        x, t = _rows(x, MLP_IN, "x"), _rows(t, MLP_OUT, "t")
+        if t.shape[0] != x.shape[0]:
+            raise ValueError(f"{x.shape[0]} feature rows but {t.shape[0]} target rows")
         g = np.zeros(self.n_params, np.float32)
         loss = C.c_double()
         self._ck(self.lib.pgpu_mlp_gradient(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0],
@@ -635,7 +650,9 @@ class Mlp:
         return loss.value, g
 
     def set_dataset(self, x, t):
-        x, t = _f32(x), _f32(t)
+        x, t = _rows(x, MLP_IN, "x"), _rows(t, MLP_OUT, "t")
+        if t.shape[0] != x.shape[0]:
+            raise ValueError(f"{x.shape[0]} feature rows but {t.shape[0]} target rows")
         self._ck(self.lib.pgpu_mlp_set_dataset(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0]))
 
     def add_samples(self, ctx: Context, n: int, seed: int = 0):
@@ -647,8 +664,8 @@ class Mlp:
 
     def dataset(self, max_rows: int | None = None):
         n = self.rows if max_rows is None else min(max_rows, self.rows)
-        x = np.zeros((n, 24), np.float32)
-        t = np.zeros((n, 6), np.float32)
+        x = np.zeros((n, MLP_IN), np.float32)
+        t = np.zeros((n, MLP_OUT), np.float32)
         self._ck(self.lib.pgpu_mlp_get_dataset(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), n))
         return x, t
 

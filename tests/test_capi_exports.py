@@ -74,3 +74,14 @@ def test_surrogate_config_defaults_and_unknown_settings():
     assert cfg.tolerance == 1e-4 and cfg.leaf_size == 256 and cfg.check_targets == 4096
     with pytest.raises(TypeError, match="unknown surrogate setting 'near_width'"):
         capi.surrogate_config(near_width=4.0)
+
+
+def test_network_rows_are_checked():
+    # the network reads rows x 24 features and rows x 6 targets
+    import numpy as np
+    x = capi._rows(np.zeros((5, 24)), capi.MLP_IN, "x")
+    assert x.dtype == np.float32 and x.shape == (5, 24)
+    with pytest.raises(ValueError, match=r"x must have shape \(rows, 24\)"):
+        capi._rows(np.zeros((5, 20)), capi.MLP_IN, "x")
+    with pytest.raises(ValueError, match="must have shape"):
+        capi._rows(np.zeros(24), capi.MLP_IN, "x")
