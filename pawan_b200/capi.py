@@ -556,6 +556,8 @@ class Context:
     def set_states_flat(self, state, maxn):
         m = np.ascontiguousarray(maxn, dtype=np.int64)
         st = _c(state)
+        if st.size < 6 * int(m.sum()):
+            raise ValueError(f"the flat state holds {st.size} values; capacities {m.tolist()} need {6 * int(m.sum())}")
         self._ck(self.lib.pgpu_set_states_flat(self.h, _p(st), m.ctypes.data_as(_i64p), len(m)))
 
     def get_states_flat(self, maxn):
