@@ -417,7 +417,8 @@ int pgpu_mlp_gradient(pgpu_mlp *mlp, const float *x, const float *t, int64_t row
 /* Training set: replace with host rows, or append rows drawn from the octree
  * of a context's last surrogate evaluation (targets are the exact direct-sum
  * contribution of the cell minus its expansion to the context's surrogate
- * order, scaled). */
+ * order, scaled).  The network and the context must be on the same device
+ * (PGPU_EINVAL otherwise), here and in pgpu_surrogate_set_mlp. */
 int pgpu_mlp_set_dataset(pgpu_mlp *mlp, const float *x, const float *t, int64_t rows);
 int pgpu_mlp_add_samples(pgpu_mlp *mlp, pgpu_ctx *ctx, int64_t nsamples, int seed);
 int64_t pgpu_mlp_dataset_rows(pgpu_mlp *mlp);
